@@ -1,0 +1,285 @@
+/*
+ * ldp.h -- C ABI of the B200 trajectory engine for the single- and
+ * double-barrier Langevin models of LangevinDynamicsForPCP.
+ *
+ * Plain C types only (no CUDA or torch types): a cgo / JNI / ctypes binding
+ * can bind this header directly.  Every entry point returns an ldp_status;
+ * none of them calls exit().  The library owns device memory and job
+ * objects; the caller owns every host buffer and string it passes in.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   process entry  `mpirun ./langevinDynamics{Single,Double}Barrier -i x.inp`
+ *                  src/langevinDynamicsSingleBarrier.cpp:6-252,
+ *                  src/langevinDynamicsDoubleBarrier.cpp:6-270
+ *   plugin seam    LangevinEquationSIMDMultiple (Initialize, Integrate,
+ *                  Get*Average, GetStateCount, Write/ReadRestartFile)
+ *                  src/langevinDynamicsSingleBarrier.h:823-2770,
+ *                  src/langevinDynamicsDoubleBarrier.h:933-3410
+ *   orchestration  LangevinEquationRunnerMPI::Setup/Run
+ *                  src/langevinDynamicsSingleBarrier.h:3125-4039
+ */
+#ifndef LDP_H
+#define LDP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDP_ABI_VERSION 1
+#define LDP_MAX_CG 16      /* FPTCG entries accepted per job              */
+#define LDP_PATH_MAX 512   /* OUTPUTBASE / restart base name buffer sizes */
+
+typedef enum ldp_status {
+    LDP_OK = 0,
+    LDP_ERR_INVALID = 1,     /* bad argument or inconsistent parameters      */
+    LDP_ERR_NOMEM = 2,       /* device or host allocation failed / too large */
+    LDP_ERR_DEVICE = 3,      /* CUDA error, or the CUDA library is missing   */
+    LDP_ERR_TIMEOUT = 4,     /* a bounded wait ran out                       */
+    LDP_ERR_IO = 5,          /* file could not be opened / written           */
+    LDP_ERR_PARSE = 6,       /* .inp grammar or option error                 */
+    LDP_ERR_UNSUPPORTED = 7, /* option combination not implemented           */
+    LDP_ERR_NOT_READY = 8,   /* results asked for before the job finished    */
+    LDP_ERR_RESTART = 9      /* restart file missing, corrupt or mismatched  */
+} ldp_status;
+
+typedef enum ldp_model { LDP_MODEL_SINGLE = 0, LDP_MODEL_DOUBLE = 1 } ldp_model;
+
+typedef enum ldp_precision {
+    LDP_PREC_FP64_PLAIN = 0,   /* FP64 state, one trajectory per thread      */
+    LDP_PREC_FP32_BATCHED = 1  /* FP32 cell-local state, persistent kernel   */
+} ldp_precision;
+
+typedef enum ldp_mode {
+    LDP_MODE_FIXED_STEPS = 0,   /* reference semantics: NUMBEROFSTEPS steps,
+                                   renewal events recorded on the way        */
+    LDP_MODE_FIRST_PASSAGE = 1  /* run each trajectory to its first
+                                   bottom-to-different-bottom passage (FPT2
+                                   event), capped at step_cap (censored)     */
+} ldp_mode;
+
+/*
+ * One .inp file.  Field names follow the .inp keys; defaults are those of
+ * the reference's AddOption calls (ldp_params_default).
+ * Single model: barrier_heights[0][s] = BARRIERHEIGHTS s (state s),
+ *               barrier_half_width[0] = BARRIERHALFWIDTH.
+ * Double model: barrier_heights[b][s] = BARRIERHEIGHTSb s,
+ *               barrier_half_width[b] = BARRIERHALFWIDTHb,
+ *               barrier_position[b]   = BARRIERPOSITIONb.
+ */
+typedef struct ldp_params {
+    int32_t model;                 /* ldp_model                              */
+    int32_t overdamped;            /* OVERDAMPED                             */
+    double x0, v0, gamma, kb, temperature, mass; /* X0 V0 GAMMA KB TEMPERATURE MASS */
+    int32_t randomize_v;           /* RANDOMIZEV                             */
+    double periodic_length;        /* PERIODICLENGTH                         */
+    double barrier_heights[2][2];  /* see above                              */
+    double barrier_half_width[2];
+    double barrier_position[2];
+    double timestep;               /* TIMESTEP                               */
+    uint64_t number_of_steps;      /* NUMBEROFSTEPS                          */
+    uint64_t number_of_previous_steps; /* NUMBEROFPREVIOUSSTEPS              */
+    int32_t number_of_runs;        /* NUMBEROFRUNS (trials)                  */
+    uint64_t freq_save;            /* FREQSAVE                               */
+    uint64_t freq_stat;            /* FREQSTAT (accepted, ignored as in the reference) */
+    int32_t distribution_v0;       /* DISTRIBUTIONV0                         */
+    int32_t distribution_s0;       /* DISTRIBUTIONS0                         */
+    double tau;                    /* TAU                                    */
+    int32_t initial_state;         /* INITIALSTATE                           */
+    int32_t randomize_states;      /* RANDOMIZESTATES                        */
+    int32_t uniform_initial_states;/* UNIFORMINITALSTATES                    */
+    int32_t eq;                    /* EQ (first value)                       */
+    double eq_constant;            /* EQ (second value), K                   */
+    int32_t waiting_time;          /* WAITINGTIME                            */
+    int32_t fpt;                   /* FPT                                    */
+    int32_t tpt;                   /* TPT                                    */
+    int32_t fptcg;                 /* FPTCG flag (last entry's boolean)      */
+    int32_t n_cg;                  /* number of FPTCG entries                */
+    int32_t cg_sizes[LDP_MAX_CG];  /* FPTCG sizes                            */
+    int32_t read_restart;          /* READRESTART                            */
+    int32_t write_restart;         /* WRITERESTART                           */
+    char input_restart[LDP_PATH_MAX];   /* INPUTRESTART                      */
+    char output_restart[LDP_PATH_MAX];  /* OUTPUTRESTART                     */
+    char output_base[LDP_PATH_MAX];     /* OUTPUTBASE                        */
+    int32_t write_x;               /* WRITEX                                 */
+    uint64_t number_of_log_samples;/* NUMBEROFLOGSAMPLES                     */
+    int64_t random_seed;           /* RANDOMSEED (-1: time based)            */
+    int32_t print_timer;           /* PRINTTIMER                             */
+} ldp_params;
+
+/* How a job is laid out and executed.  ntraj = ranks * runs * lanes. */
+typedef struct ldp_job_opts {
+    int32_t lanes;            /* trajectories per (rank, trial): the reference's
+                                 SIMD width; default 8 (AVX-512 build)       */
+    int32_t ranks;            /* virtual ranks (the reference's mpirun -n);
+                                 default 1                                   */
+    int32_t precision;        /* ldp_precision; default FP64_PLAIN           */
+    int32_t mode;             /* ldp_mode; default FIXED_STEPS               */
+    uint64_t step_cap;        /* FIRST_PASSAGE: max steps per trajectory     */
+    int32_t table_slots;      /* per-trajectory cell-table ring slots (power
+                                 of two, >= 16); default 256                 */
+    int64_t tick_cap;         /* waiting-time ticks kept per trajectory;
+                                 -1 = automatic, 0 = none                    */
+    uint32_t job_id;          /* second Philox key word; default 0           */
+    uint64_t steps_per_launch;/* 0 = automatic                               */
+    int32_t block_size;       /* 0 = automatic                               */
+    int32_t keep_frames;      /* keep x frames on the device after the MSD
+                                 (needed for ldp_job_traj_results frames);
+                                 default 1                                   */
+} ldp_job_opts;
+
+/* Per-trajectory counters, laid out [field][ntraj]. */
+enum ldp_count_field {
+    LDP_C_FPT = 0,   /* bottom -> barrier top events                         */
+    LDP_C_FPT2,      /* bottom -> different bottom events                    */
+    LDP_C_TPT,       /* transition path (bottom -> top) events               */
+    LDP_C_TPT2,      /* transition path (bottom -> other bottom) events      */
+    LDP_C_INIT0,     /* FPT events whose initial barrier state was 0         */
+    LDP_C_INIT1,     /* ... was 1                                            */
+    LDP_C_INST0,     /* FPT events whose instantaneous barrier state was 0   */
+    LDP_C_INST1,     /* ... was 1                                            */
+    LDP_C_STATE0,    /* steps spent in state 0 (step 0 included)             */
+    LDP_C_STATE1,    /* steps spent in state 1                               */
+    LDP_C_WT,        /* waiting-time ticks recorded (may exceed tick_cap)    */
+    LDP_C_EVICT,     /* cell-table ring evictions                            */
+    LDP_C_FLAGS,     /* LDP_FLAG_* bits                                      */
+    LDP_C_STEPS,     /* steps integrated by this trajectory                  */
+    LDP_C_CG0,       /* FPTCG events, LDP_C_CG0 + j for FPTCG entry j        */
+    LDP_NCOUNT = LDP_C_CG0 + LDP_MAX_CG
+};
+
+/* Per-trajectory event-time sums (FP64, event order), [field][ntraj]. */
+enum ldp_sum_field {
+    LDP_S_FPT = 0, LDP_S_FPT2, LDP_S_TPT, LDP_S_TPT2,
+    LDP_S_CG0,       /* LDP_S_CG0 + j */
+    LDP_NSUM = LDP_S_CG0 + LDP_MAX_CG
+};
+
+#define LDP_FLAG_NONFINITE 1u   /* x became NaN/inf; trajectory frozen        */
+#define LDP_FLAG_TICK_OVERFLOW 2u /* more waiting ticks than tick_cap          */
+#define LDP_FLAG_CENSORED 4u    /* FIRST_PASSAGE: step_cap reached, no event  */
+
+typedef struct ldp_job_info {
+    int64_t ntraj;        /* trajectories                                   */
+    int64_t nframe;       /* frames per trajectory (NUMBEROFSTEPS/FREQSAVE+1) */
+    int64_t nlag;         /* MSD lag points                                  */
+    int64_t steps;        /* steps integrated per trajectory (fixed mode)    */
+    int64_t tick_cap;     /* waiting ticks kept per trajectory               */
+    int32_t n_cg;
+    int32_t precision;
+    int32_t mode;
+    int32_t done;
+} ldp_job_info;
+
+/*
+ * Caller-allocated host buffers for per-trajectory results; any pointer may
+ * be NULL to skip that array.  Frame arrays are [nframe][ntraj].
+ */
+typedef struct ldp_traj_results {
+    int64_t *counts;        /* [LDP_NCOUNT][ntraj]                          */
+    double  *sums;          /* [LDP_NSUM][ntraj]                            */
+    int32_t *state0;        /* initial barrier state                        */
+    double  *v0;            /* initial velocity instance                    */
+    double  *x_final;       /* position after the last step                 */
+    double  *v_final;
+    int32_t *state_final;
+    int64_t *ticks;         /* [ntraj][tick_cap] waiting-time ticks (steps) */
+    double  *frames_x;      /* [nframe][ntraj]                              */
+    double  *frames_v, *frames_f, *frames_barrier, *frames_pe, *frames_ke,
+            *frames_state;  /* WRITEX series, [nframe][ntraj]               */
+} ldp_traj_results;
+
+typedef struct ldp_timing {
+    double integrate_ms;    /* device time of the trajectory kernels         */
+    double msd_ms;          /* device time of the MSD kernels                */
+    double reduce_ms;       /* device time of the reduction kernels          */
+    int64_t launches;       /* kernels launched                              */
+    int64_t particle_steps; /* trajectory-steps integrated                   */
+} ldp_timing;
+
+typedef struct ldp_ctx ldp_ctx;
+typedef struct ldp_job ldp_job;
+
+/* Library / context.  Replaces MPIKERNEL::MPIKernel + runner construction
+ * (src/mpiKernel.cpp:1-60, src/langevinDynamicsSingleBarrier.h:2890-3038). */
+int         ldp_abi_version(void);
+ldp_status  ldp_create(ldp_ctx **out, int device);
+void        ldp_destroy(ldp_ctx *ctx);
+const char *ldp_last_error(const ldp_ctx *ctx);
+const char *ldp_status_string(ldp_status st);
+
+/* Launch shape of the FP32 batched persistent kernel in this context:
+ * threads per block, resident blocks per SM (0: as many as fit), step pairs
+ * per slot and launch, and cell-table ring slots per resident slot (power of
+ * two).  Zero keeps the default.  Must precede the context's first FP32
+ * job.  No reference counterpart (the reference has no GPU launch). */
+ldp_status  ldp_ctx_set_fp32_shape(ldp_ctx *ctx, int block, int blocks_per_sm, uint64_t pair_budget,
+                                   int ring_slots);
+/* Device-time markers on the context's stream (16 slots): record a marker,
+ * then read the elapsed device time between two markers (waits for the
+ * second).  They replace the reference's wall-clock timers around Integrate
+ * (clsSystemTimeCPP, src/langevinDynamicsSingleBarrier.h:3416-3448). */
+ldp_status  ldp_ctx_mark(ldp_ctx *ctx, int mark);
+ldp_status  ldp_ctx_elapsed_ms(ldp_ctx *ctx, int mark_a, int mark_b, double *ms);
+ldp_status  ldp_ctx_synchronize(ldp_ctx *ctx);
+/* The shape in effect: the resolved values once the first FP32 job ran. */
+ldp_status  ldp_ctx_get_fp32_shape(ldp_ctx *ctx, int *block, int *grid, uint64_t *pair_budget,
+                                   int *ring_slots);
+
+/* Parameters.  Replaces INPUTPARSER::InputParser::AddOption/Parse/
+ * GetOptionValue (src/inputParser.cpp:45-330) as used by the two mains
+ * (src/langevinDynamicsSingleBarrier.cpp:64-188). */
+void        ldp_params_default(int model, ldp_params *p);
+ldp_status  ldp_params_from_inp(const char *path, int model, ldp_params *p,
+                                char *err, size_t errlen);
+ldp_status  ldp_params_from_inp_text(const char *text, const char *base_dir,
+                                     int model, ldp_params *p,
+                                     char *err, size_t errlen);
+/* Writes the default .inp (the reference's `-o file.inp`,
+ * src/inputParser.cpp:212-266). */
+ldp_status  ldp_write_default_inp(const char *path, int model);
+
+/* Jobs.  Replaces LangevinEquationSIMDMultiple::Initialize/Integrate and the
+ * trial loop of LangevinEquationRunnerMPI::Run
+ * (src/langevinDynamicsSingleBarrier.h:1276, 1386, 3429-3589). */
+void        ldp_job_opts_default(ldp_job_opts *o);
+ldp_status  ldp_job_create(ldp_ctx *ctx, const ldp_params *p,
+                           const ldp_job_opts *o, ldp_job **out);
+ldp_status  ldp_job_set_precision(ldp_job *job, int precision);
+ldp_status  ldp_submit(ldp_ctx *ctx, ldp_job *job);   /* asynchronous      */
+/* Submits several jobs at once: all FP32 batched jobs are registered in the
+ * work queue before any launch, so their trajectories share every persistent
+ * launch (the reference runs one .inp per mpirun; no counterpart). */
+ldp_status  ldp_submit_batch(ldp_ctx *ctx, ldp_job **jobs, int njobs);
+ldp_status  ldp_poll(ldp_ctx *ctx, ldp_job *job, int *done);
+ldp_status  ldp_wait(ldp_ctx *ctx, ldp_job *job);
+ldp_status  ldp_job_info_get(const ldp_job *job, ldp_job_info *info);
+ldp_status  ldp_job_timing_get(const ldp_job *job, ldp_timing *t);
+void        ldp_job_destroy(ldp_job *job);
+
+/* Results.  Replaces the getters GetFirstPassageTimeAverage{,2},
+ * GetTransitionPathTimeAverage{,2}, GetFirstPassageTimeCGAverage2,
+ * GetStateCount, GetBarrierTick, GetX
+ * (src/langevinDynamicsSingleBarrier.h:2632-2769). */
+ldp_status  ldp_job_traj_results(ldp_job *job, ldp_traj_results *out);
+/* MSD over all trajectories (MeanSquareDisplacementBruteForce summed and
+ * divided by nrun, src/langevinDynamicsSingleBarrier.h:24-45, 3452-3461,
+ * 3893-3912); lags in frames. */
+ldp_status  ldp_job_msd(ldp_job *job, int64_t *lags, double *msd, int64_t nlag);
+/* Per-trajectory MSD before the sum over trajectories (the reference's msd0
+ * of one lane, S.h:3454-3455), [nlag][ntraj]. */
+ldp_status  ldp_job_msd_traj(ldp_job *job, double *msd0);
+/* Writes the reference's output files under dir (NULL: current directory):
+ * src/langevinDynamicsSingleBarrier.h:3594-4036. */
+ldp_status  ldp_job_write_outputs(ldp_job *job, const char *dir);
+
+/* One-shot drop-in for `mpirun -n ranks ./exe -i path`. */
+ldp_status  ldp_run_inp(ldp_ctx *ctx, const char *path, int model,
+                        const ldp_job_opts *o, const char *outdir);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LDP_H */

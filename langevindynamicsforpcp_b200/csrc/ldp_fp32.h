@@ -1,0 +1,86 @@
+// ldp_fp32.h -- FP32 batched persistent runtime: job table, work queue and
+// slot state shared by the host scheduler and the persistent kernel.
+//
+// A "job" is one parameter set (one .inp) with its own output arrays; its
+// trajectories are the work items.  Jobs of one model type (single/double x
+// overdamped/underdamped) share one persistent kernel instance and one work
+// queue.  Each resident thread ("slot") owns one trajectory at a time, holds
+// its hot state in registers, and pulls the next trajectory from the queue
+// when its trajectory retires (warp-aggregated claim).  Results never depend
+// on which slot ran a trajectory: every random draw is keyed by
+// (seed, job id, trajectory, step).
+#pragma once
+#include <cstdint>
+#include "ldp_engine.h"
+
+namespace ldp {
+
+constexpr int kFp32MaxJobs = 16384;     // resident jobs per queue
+constexpr int kFp32MaxRanges = 16384;   // published item ranges per queue
+
+// Per-job constants and output pointers (device resident, one per job).
+struct JobF {
+    // model switches (jobs of one queue share dbl/over)
+    int32_t eta, eq, rs, rv, us, init_state, wt, fpt, tpt, cg, n_cg, write_x, at_bottom, fp_mode;
+    int32_t lanes, nruns, slots_log2, pad0;
+    int32_t cg_size[LDP_MAX_CG];
+    uint32_t key0, key1;
+    // FP32 step constants
+    float L, halfL, w, slope[2], xb[2], lo0, hi1, xc, sN[2][2], sP[2][2];
+    float c_drift, sig_r, hdt_invM, hdt, expg, sig_v;
+    // FP64 constants (step 0, events, frames)
+    double x0, v0, dt, Ld, invL, sig_v0, sig_r_d, a_lap, c_lap[2], p_first, p_cell0, mhalf;
+    double Hs[2], Hd[2][2], iN[2][2], iP[2][2], sNd[2][2], sPd[2][2], wd, xbd[2], lo0d, hi1d, xcd;
+    uint64_t T_eq, T_as[2];
+    uint64_t nsteps, freq_save;
+    int64_t nframe, tick_cap, ntraj;
+    // per-trajectory outputs [field][ntraj] (job local)
+    int64_t* counts;     // [LDP_NCOUNT][ntraj]
+    int64_t* ssum;       // [LDP_NSUM][ntraj] event durations in steps
+    int32_t* state0;
+    double *v0s, *x_final, *v_final;
+    int32_t* state_final;
+    int64_t* ticks;      // [ntraj][tick_cap]
+    double *fx, *fv, *ff, *fb, *fpe, *fke, *fst;  // frames [nframe][ntraj]
+    // per-trajectory cold statistics state (touched only on events)
+    int32_t* bits;
+    int64_t *fpt_last, *fpt2_last, *tpt_last, *tpt2_last, *wt_tick;
+    int32_t *init_idx0, *init_idx1, *idx2_0, *idx2_1, *tpt2_well;
+    int64_t* cg_last;    // [LDP_MAX_CG][ntraj]
+    int32_t* cg_well;    // [LDP_MAX_CG][ntraj]
+    unsigned long long* remaining;   // trajectories of this job not yet retired
+};
+
+// A work queue: published item ranges (job index, trajectory count) with
+// inclusive prefix ends; head is claimed by the kernel, tail by the host.
+struct QueueDev {
+    int64_t* range_end;     // [kFp32MaxRanges] prefix sums of published items
+    int32_t* range_job;     // [kFp32MaxRanges]
+    int64_t* range_first;   // [kFp32MaxRanges] first trajectory of the range
+    unsigned long long* head;  // claimed items
+    unsigned long long* tail;  // published items (written by the host)
+    int32_t* nranges;       // published ranges (written by the host)
+    JobF* jobs;             // [kFp32MaxJobs]
+};
+
+// Per-slot state saved between launches, [nslots].
+struct SlotsDev {
+    int64_t nslots;
+    int32_t* job;           // -1: no trajectory
+    int64_t* traj;
+    int64_t* step;          // next step to integrate
+    float *xp, *rv;         // rv: R_prev (overdamped) or v (underdamped)
+    int32_t *cell, *st;     // st: state | lb << 1
+    int64_t *sc0, *sc1;
+    int64_t* ring_tag;      // [R][nslots]
+    int64_t* ring_data;
+    unsigned long long* retired;   // total retired trajectories (all jobs)
+    int32_t ring_slots;
+};
+
+// Resident blocks per SM of the persistent kernel (0 on error).
+int fp32_blocks_per_sm(bool dbl, bool over, int block);
+int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint64_t pair_budget,
+                           int grid, int block, void* stream);
+
+}  // namespace ldp

@@ -1,0 +1,318 @@
+// ldp_fp32_rt.cu -- host side of the FP32 batched persistent path.
+//
+// One work queue and one set of persistent slots per model type
+// (single/double x overdamped/underdamped), created on first use in a
+// context.  Submitting an FP32 job writes its JobF into the queue's device
+// job table, publishes its trajectories as one item range, and enqueues
+// persistent-kernel launches; completion is the job's device "remaining"
+// counter reaching zero.  The job scheduler (mpiKernel's role in the
+// reference, src/mpiKernel.cpp) is this queue: trajectories of many jobs
+// share every launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "ldp_fp32.h"
+#include "ldp_internal.h"
+
+namespace ldp {
+int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
+               double* msd0, double* msd_sum, void* stream);
+
+struct Fp32Queue {
+    bool ready = false;
+    QueueDev q{};
+    SlotsDev s{};
+    void* qmem = nullptr;
+    void* smem = nullptr;
+    int grid = 0, block = 256;
+    uint64_t pair_budget = 1 << 15;
+    int64_t nranges = 0;
+    unsigned long long tail = 0;
+    int64_t* h_stage = nullptr;   // pinned staging for range/tail uploads
+    std::vector<ldp_job*> table;  // job table slot -> job
+    std::vector<int> free_slots;
+};
+
+struct Fp32Runtime {
+    Fp32Queue q[4];
+};
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
+    if (Q.ready) return 0;
+    Q.block = ctx->fp32_block ? ctx->fp32_block : 256;
+    // A persistent grid never exceeds what is resident at once.
+    const int resident = fp32_blocks_per_sm(type >= 2, (type & 1) != 0, Q.block);
+    int bps = ctx->fp32_blocks_per_sm ? ctx->fp32_blocks_per_sm : resident;
+    if (resident > 0) bps = std::min(bps, resident);
+    bps = std::max(bps, 1);
+    Q.grid = ctx->sm_count * bps;
+    Q.pair_budget = ctx->fp32_pair_budget ? ctx->fp32_pair_budget : (1u << 15);
+    const int64_t nslots = (int64_t)Q.grid * Q.block;
+    // queue + job table
+    size_t qb = al256(sizeof(int64_t) * kFp32MaxRanges) * 2 + al256(sizeof(int32_t) * kFp32MaxRanges) +
+                al256(sizeof(unsigned long long) * 2) + al256(sizeof(int32_t)) + al256(sizeof(JobF) * kFp32MaxJobs);
+    cudaError_t e = cudaMalloc(&Q.qmem, qb);
+    if (e != cudaSuccess) return (int)e;
+    cudaMemset(Q.qmem, 0, qb);
+    char* a = (char*)Q.qmem;
+    size_t o = 0;
+    Q.q.range_end = (int64_t*)(a + o); o += al256(sizeof(int64_t) * kFp32MaxRanges);
+    Q.q.range_first = (int64_t*)(a + o); o += al256(sizeof(int64_t) * kFp32MaxRanges);
+    Q.q.range_job = (int32_t*)(a + o); o += al256(sizeof(int32_t) * kFp32MaxRanges);
+    Q.q.head = (unsigned long long*)(a + o);
+    Q.q.tail = Q.q.head + 1;
+    o += al256(sizeof(unsigned long long) * 2);
+    Q.q.nranges = (int32_t*)(a + o); o += al256(sizeof(int32_t));
+    Q.q.jobs = (JobF*)(a + o);
+    // slots
+    const int R = ring_slots;
+    size_t sb = al256(sizeof(int32_t) * nslots) * 3 + al256(sizeof(int64_t) * nslots) * 4 +
+                al256(sizeof(float) * nslots) * 2 + al256(sizeof(int64_t) * (size_t)R * nslots) * 2 +
+                al256(sizeof(unsigned long long));
+    e = cudaMalloc(&Q.smem, sb);
+    if (e != cudaSuccess) return (int)e;
+    cudaMemset(Q.smem, 0, sb);
+    a = (char*)Q.smem;
+    o = 0;
+    SlotsDev& S = Q.s;
+    S.nslots = nslots;
+    S.ring_slots = R;
+    S.job = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.cell = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.st = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.traj = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.step = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.sc0 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.sc1 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.xp = (float*)(a + o); o += al256(sizeof(float) * nslots);
+    S.rv = (float*)(a + o); o += al256(sizeof(float) * nslots);
+    S.ring_tag = (int64_t*)(a + o); o += al256(sizeof(int64_t) * (size_t)R * nslots);
+    S.ring_data = (int64_t*)(a + o); o += al256(sizeof(int64_t) * (size_t)R * nslots);
+    S.retired = (unsigned long long*)(a + o);
+    // every slot starts empty
+    std::vector<int32_t> neg((size_t)nslots, -1);
+    cudaMemcpy(S.job, neg.data(), sizeof(int32_t) * nslots, cudaMemcpyHostToDevice);
+    e = cudaMallocHost((void**)&Q.h_stage, 4096);
+    if (e != cudaSuccess) return (int)e;
+    Q.table.assign(kFp32MaxJobs, nullptr);
+    Q.free_slots.clear();
+    for (int i = kFp32MaxJobs - 1; i >= 0; --i) Q.free_slots.push_back(i);
+    Q.ready = true;
+    return 0;
+}
+
+static void fill_jobf(const ldp_job* job, JobF* J) {
+    std::memset(J, 0, sizeof(*J));
+    const KConst& k = job->k;
+    const TrajState& S = job->st;
+    const int64_t n = job->ntraj;
+    J->eta = k.eta; J->eq = k.eq; J->rs = k.rs; J->rv = k.rv; J->us = k.us; J->init_state = k.init_state;
+    J->wt = k.wt; J->fpt = k.fpt; J->tpt = k.tpt; J->cg = k.cg; J->n_cg = k.n_cg; J->write_x = k.write_x;
+    J->at_bottom = k.at_bottom; J->fp_mode = k.fp_mode; J->lanes = k.lanes; J->nruns = k.nruns;
+    for (int j = 0; j < LDP_MAX_CG; ++j) J->cg_size[j] = k.cg_size[j] ? k.cg_size[j] : 1;
+    J->key0 = k.key0; J->key1 = k.key1;
+    J->L = k.fL; J->halfL = k.fhalfL; J->w = k.fw;
+    J->slope[0] = k.fslope[0]; J->slope[1] = k.fslope[1];
+    J->xb[0] = k.fxb[0]; J->xb[1] = k.fxb[1]; J->lo0 = k.flo0; J->hi1 = k.fhi1; J->xc = k.fxc;
+    for (int b = 0; b < 2; ++b)
+        for (int s = 0; s < 2; ++s) {
+            J->sN[b][s] = k.fsN[b][s]; J->sP[b][s] = k.fsP[b][s];
+            J->sNd[b][s] = k.sN[b][s]; J->sPd[b][s] = k.sP[b][s];
+            J->Hd[b][s] = k.Hd[b][s]; J->iN[b][s] = k.iN[b][s]; J->iP[b][s] = k.iP[b][s];
+        }
+    J->c_drift = k.fc_drift; J->sig_r = k.fsig_r; J->hdt_invM = k.fhdt_invM; J->hdt = k.fhdt;
+    J->expg = k.fexpg; J->sig_v = k.fsig_v;
+    J->x0 = k.x0; J->v0 = k.v0; J->dt = k.dt; J->Ld = k.L; J->invL = k.invL; J->sig_v0 = k.sig_v0;
+    J->sig_r_d = k.sig_r; J->a_lap = k.a_lap; J->c_lap[0] = k.c_lap[0]; J->c_lap[1] = k.c_lap[1];
+    J->p_first = k.p_first; J->p_cell0 = k.p_cell0; J->mhalf = k.mhalf;
+    J->Hs[0] = k.Hs[0]; J->Hs[1] = k.Hs[1]; J->wd = k.w;
+    J->xbd[0] = k.xb[0]; J->xbd[1] = k.xb[1]; J->lo0d = k.lo0; J->hi1d = k.hi1; J->xcd = k.xc;
+    J->T_eq = k.T_eq; J->T_as[0] = k.T_as[0]; J->T_as[1] = k.T_as[1];
+    J->nsteps = job->nsteps;
+    J->freq_save = k.freq_save;
+    J->nframe = k.nframe;
+    J->tick_cap = job->o.tick_cap;
+    J->ntraj = n;
+    J->counts = S.counts;
+    J->ssum = job->d_ssum;
+    J->state0 = S.state0;
+    J->v0s = S.v0;
+    J->x_final = S.x;
+    J->v_final = S.v;
+    J->state_final = S.state;
+    J->ticks = S.ticks;
+    J->fx = S.fx; J->fv = S.fv; J->ff = S.ff; J->fb = S.fb; J->fpe = S.fpe; J->fke = S.fke; J->fst = S.fst;
+    J->bits = S.bits;
+    // 64-bit step clocks reuse the FP64 arrays of the arena.
+    J->fpt_last = (int64_t*)S.fpt_last;
+    J->fpt2_last = (int64_t*)S.fpt2_last;
+    J->tpt_last = (int64_t*)S.tpt_last;
+    J->tpt2_last = (int64_t*)S.tpt2_last;
+    J->wt_tick = S.wt_tick;
+    int32_t* b = job->d_i32b;
+    J->init_idx0 = b; J->init_idx1 = b + n; J->idx2_0 = b + 2 * n; J->idx2_1 = b + 3 * n; J->tpt2_well = b + 4 * n;
+    J->cg_well = b + 5 * n;
+    J->cg_last = S.cg_well;   // int64 [ncg][n]
+    J->remaining = (unsigned long long*)job->d_aux;
+}
+
+int fp32_type_of(const ldp_job* job) { return (job->k.dbl ? 2 : 0) + (job->k.over ? 1 : 0); }
+
+static Fp32Runtime* runtime(ldp_ctx* ctx) {
+    if (!ctx->fp32) ctx->fp32 = new Fp32Runtime();
+    return ctx->fp32;
+}
+
+// Registers the job and publishes its trajectories.
+int fp32_register(ldp_job* job) {
+    ldp_ctx* ctx = job->ctx;
+    cudaStream_t st = ctx->stream;
+    Fp32Runtime* rt = runtime(ctx);
+    const int type = fp32_type_of(job);
+    Fp32Queue& Q = rt->q[type];
+    int e = queue_init(ctx, Q, type, ctx->fp32_ring_slots ? ctx->fp32_ring_slots : 64);
+    if (e) return e;
+    if (Q.free_slots.empty() || Q.nranges >= kFp32MaxRanges) return (int)cudaErrorMemoryAllocation;
+    const int slot = Q.free_slots.back();
+    Q.free_slots.pop_back();
+    Q.table[slot] = job;
+    job->fp32_type = type;
+    job->fp32_slot = slot;
+    JobF J;
+    fill_jobf(job, &J);
+    // The JobF and the range are staged in pinned memory so the copies stay
+    // asynchronous; the stage is reused only after the stream has drained it.
+    cudaStreamSynchronize(st);
+    static_assert(sizeof(JobF) <= 4096 - 64, "JobF must fit the staging buffer");
+    std::memcpy(Q.h_stage + 8, &J, sizeof(J));
+    unsigned long long remaining = (unsigned long long)job->ntraj;
+    Q.h_stage[0] = (int64_t)remaining;
+    cudaMemcpyAsync(J.remaining, &Q.h_stage[0], sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&Q.q.jobs[slot], Q.h_stage + 8, sizeof(J), cudaMemcpyHostToDevice, st);
+    const int64_t r = Q.nranges;
+    Q.tail += (unsigned long long)job->ntraj;
+    Q.h_stage[1] = (int64_t)Q.tail;       // range_end
+    Q.h_stage[2] = 0;                      // range_first
+    Q.h_stage[3] = slot;                   // range_job (low 32 bits)
+    Q.h_stage[4] = r + 1;                  // nranges
+    Q.h_stage[5] = (int64_t)Q.tail;        // tail
+    cudaMemcpyAsync(&Q.q.range_end[r], &Q.h_stage[1], sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&Q.q.range_first[r], &Q.h_stage[2], sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&Q.q.range_job[r], &Q.h_stage[3], sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(Q.q.nranges, &Q.h_stage[4], sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(Q.q.tail, &Q.h_stage[5], sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    Q.nranges = r + 1;
+    return (int)cudaGetLastError();
+}
+
+// Enqueues nlaunch persistent-kernel launches of the job's queue.
+int fp32_pump(ldp_job* job, int nlaunch) {
+    ldp_ctx* ctx = job->ctx;
+    Fp32Queue& Q = ctx->fp32->q[job->fp32_type];
+    const bool dbl = job->k.dbl, over = job->k.over;
+    for (int i = 0; i < nlaunch; ++i) {
+        int e = launch_fp32_persistent(dbl, over, Q.q, Q.s, Q.pair_budget, Q.grid, Q.block, ctx->stream);
+        if (e) return e;
+        ++job->launches;
+    }
+    return 0;
+}
+
+// Launches needed for the job's queue to drain, assuming it runs alone.
+int fp32_estimate_launches(const ldp_job* job) {
+    const Fp32Queue& Q = job->ctx->fp32->q[job->fp32_type];
+    const double pairs = (double)job->ntraj * (double)((job->nsteps + 1) / 2);
+    const double cap = (double)Q.s.nslots * (double)Q.pair_budget;
+    int n = (int)(pairs / cap) + 1;
+    if (job->o.mode == LDP_MODE_FIRST_PASSAGE) n = std::max(1, n / 8);
+    return std::min(n, 4096);
+}
+
+int fp32_remaining(ldp_job* job, unsigned long long* rem) {
+    return (int)cudaMemcpy(rem, job->d_aux, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+}
+
+__global__ void ssum_to_time_kernel(const int64_t* ssum, double* sums, double dt, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sums[i] = dt * (double)ssum[i];
+}
+
+// Post-processing after all trajectories retired: event-duration sums in
+// time units, then the MSD of the saved frames.
+int fp32_finalize(ldp_job* job) {
+    cudaStream_t st = job->ctx->stream;
+    const int64_t n = (int64_t)LDP_NSUM * job->ntraj;
+    ssum_to_time_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(job->d_ssum, job->st.sums, job->k.dt, n);
+    int e = (int)cudaGetLastError();
+    if (e) return e;
+    ++job->launches;
+    if (job->o.mode == LDP_MODE_FIXED_STEPS && !job->lags.empty()) {
+        e = launch_msd(job->st.fx, job->nframe, job->ntraj, job->d_lags, (int64_t)job->lags.size(), job->d_msd0,
+                       job->d_msd, st);
+        if (e) return e;
+        job->launches += 2;
+    }
+    return 0;
+}
+
+void fp32_release(ldp_job* job) {
+    if (job->fp32_slot < 0 || !job->ctx->fp32) return;
+    Fp32Queue& Q = job->ctx->fp32->q[job->fp32_type];
+    Q.table[job->fp32_slot] = nullptr;
+    Q.free_slots.push_back(job->fp32_slot);
+    job->fp32_slot = -1;
+}
+
+void fp32_destroy_runtime(ldp_ctx* ctx) {
+    if (!ctx->fp32) return;
+    for (auto& Q : ctx->fp32->q) {
+        if (Q.qmem) cudaFree(Q.qmem);
+        if (Q.smem) cudaFree(Q.smem);
+        if (Q.h_stage) cudaFreeHost(Q.h_stage);
+    }
+    delete ctx->fp32;
+    ctx->fp32 = nullptr;
+}
+
+}  // namespace ldp
+
+extern "C" ldp_status ldp_ctx_set_fp32_shape(ldp_ctx* ctx, int block, int blocks_per_sm, uint64_t pair_budget,
+                                             int ring_slots) {
+    if (!ctx) return LDP_ERR_INVALID;
+    if (ctx->fp32) {
+        ldp_set_error(ctx, "the FP32 launch shape is fixed once the context ran an FP32 job");
+        return LDP_ERR_INVALID;
+    }
+    if (block < 0 || (block && (block % 32 || block > 256)) || blocks_per_sm < 0 ||
+        (ring_slots && (ring_slots < 16 || (ring_slots & (ring_slots - 1))))) {
+        ldp_set_error(ctx, "invalid FP32 shape: block %d (multiple of 32, <= 256), ring %d (power of two >= 16)",
+                      block, ring_slots);
+        return LDP_ERR_INVALID;
+    }
+    ctx->fp32_block = block;
+    ctx->fp32_blocks_per_sm = blocks_per_sm;
+    ctx->fp32_pair_budget = pair_budget;
+    ctx->fp32_ring_slots = ring_slots;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_ctx_get_fp32_shape(ldp_ctx* ctx, int* block, int* grid, uint64_t* pair_budget,
+                                             int* ring_slots) {
+    if (!ctx) return LDP_ERR_INVALID;
+    int b = ctx->fp32_block ? ctx->fp32_block : 256, g = 0;
+    uint64_t pb = ctx->fp32_pair_budget ? ctx->fp32_pair_budget : (1u << 15);
+    int r = ctx->fp32_ring_slots ? ctx->fp32_ring_slots : 64;
+    if (ctx->fp32)
+        for (auto& Q : ctx->fp32->q)
+            if (Q.ready) { b = Q.block; g = Q.grid; pb = Q.pair_budget; r = Q.s.ring_slots; break; }
+    if (block) *block = b;
+    if (grid) *grid = g;
+    if (pair_budget) *pair_budget = pb;
+    if (ring_slots) *ring_slots = r;
+    return LDP_OK;
+}

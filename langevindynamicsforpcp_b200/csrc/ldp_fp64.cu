@@ -1,0 +1,461 @@
+// ldp_fp64.cu -- plain FP64 trajectory kernels (one trajectory per thread).
+//
+// Device restatement of LangevinEquationSIMDMultiple and its overdamped
+// subclass (src/langevinDynamicsSingleBarrier.h:823-2888) and of the
+// double-barrier engine (src/langevinDynamicsDoubleBarrier.h:933-3507): the
+// per-lane SIMD loop becomes one CUDA thread per trajectory, the lane's
+// __m512d registers become this thread's registers, and the lazily grown
+// per-cell barrier table (src/DataLocator.h:100-188) becomes a tagged ring
+// of visited cells in HBM whose never-visited entries are a pure function of
+// (trajectory, cell).
+//
+// Compiled with -fmad=false: every a*b+c is two roundings unless written as
+// fma(), as in the reference's intrinsics (the only fused step is the
+// overdamped drift, _mmSIMD_fmadd_pd at S.h:2868).
+#include <cuda_runtime.h>
+#include "ldp_device.cuh"
+#include "ldp_engine.h"
+
+namespace ldp {
+
+struct T64 {
+    double x, v, F, E, rprev, barrier;
+    int64_t cell, well;
+    int lb, state;
+    uint32_t bits;
+    double fpt_last, fpt2_last, tpt_last, tpt2_last;
+    int64_t init_idx0, init_idx1, idx2_0, idx2_1, tpt2_well, wt_tick;
+};
+
+template <bool DBL>
+__device__ __forceinline__ int64_t cell_key(int64_t cell, int lb) {
+    return DBL ? cell * 2 + lb : cell;
+}
+
+// State of a cell never entered: BarrierStatus::Initialize (S.h:78-96),
+// drawn from the trajectory's TAG_CELL stream; with UNIFORMINITALSTATES the
+// value the reference hands over (S.h:1377-1380, D.h:1576-1578).
+template <bool DBL>
+__device__ int default_state(const KConst& k, uint32_t g, int64_t ck) {
+    if (k.us) {
+        if (DBL) return k.init_state;
+        const int64_t trial = ((int64_t)g / k.lanes) % k.nruns;
+        if (trial == 0) return 0;
+        if (!k.rs) return k.init_state;
+        const Words w = philox_at(0, g - (uint32_t)k.lanes, TAG_INIT, k.key0, k.key1);
+        return ((double)w.w0 * 0x1p-32 <= k.p_first) ? 0 : 1;
+    }
+    const Words w = philox_at((uint64_t)ck, g, TAG_CELL, k.key0, k.key1);
+    return ((double)w.w0 * 0x1p-32 < k.p_cell0) ? 0 : 1;
+}
+
+template <bool DBL>
+__device__ __forceinline__ void ring_load(const KConst& k, const TrajState& st, int64_t i, uint32_t g, int64_t ck,
+                                          int* state, int64_t* stamp) {
+    const int64_t slot = ck & (int64_t)(k.slots - 1);
+    const int64_t o = slot * st.n + i;
+    if (st.ring_tag[o] == ck) {
+        const int64_t d = st.ring_data[o];
+        *state = (int)(d & 1);
+        *stamp = d >> 1;
+    } else {
+        *state = default_state<DBL>(k, g, ck);
+        *stamp = 0;
+    }
+}
+
+__device__ __forceinline__ void ring_store(const KConst& k, const TrajState& st, int64_t i, int64_t ck, int state,
+                                           int64_t stamp) {
+    const int64_t slot = ck & (int64_t)(k.slots - 1);
+    const int64_t o = slot * st.n + i;
+    const int64_t old = st.ring_tag[o];
+    if (old != ck && old != INT64_MIN) st.counts[(int64_t)LDP_C_EVICT * st.n + i] += 1;
+    st.ring_tag[o] = ck;
+    st.ring_data[o] = (stamp << 1) | (int64_t)state;
+}
+
+// EnergyAndForce, S.h:1292-1324 / D.h:1464-1522.
+template <bool DBL>
+__device__ __forceinline__ void energy_force(const KConst& k, T64& t) {
+    const int s = t.state;
+    const double xp = t.x - (double)t.cell * k.L;
+    if (!DBL) {
+        const double sp = k.slope[s], sn = 0.0 - sp, H = k.Hs[s];
+        const bool onN = (xp < 0.0) && (xp > -k.w);
+        const bool onP = (xp < k.w) && (xp > 0.0);
+        double E = 0.0, F = 0.0;
+        if (onN) { E = H - xp * sn; F = sn; }
+        if (onP) { E = H - xp * sp; F = sp; }
+        t.E = E;
+        t.F = F;
+        t.barrier = H;
+    } else {
+        const bool onN0 = (xp < k.xb[0]) && (xp > k.lo0);
+        const bool onP0 = (xp < k.xc) && (xp > k.xb[0]);
+        const bool onN1 = (xp < k.xb[1]) && (xp > k.xc);
+        const bool onP1 = (xp < k.hi1) && (xp > k.xb[1]);
+        double E = 0.0, f = 0.0, B = 0.0;
+        if (onN0) { E = xp * k.sN[0][s] + k.iN[0][s]; f = k.sN[0][s]; B = k.Hd[0][s]; }
+        if (onP0) { E = xp * k.sP[0][s] + k.iP[0][s]; f = k.sP[0][s]; B = k.Hd[0][s]; }
+        if (onN1) { E = xp * k.sN[1][s] + k.iN[1][s]; f = k.sN[1][s]; B = k.Hd[1][s]; }
+        if (onP1) { E = xp * k.sP[1][s] + k.iP[1][s]; f = k.sP[1][s]; B = k.Hd[1][s]; }
+        t.E = E;
+        t.F = 0.0 - f;
+        t.barrier = B;
+    }
+}
+
+// InitializePeriodicIndices / UpdatePeriodicIndices, S.h:1838-1884,
+// D.h:2156-2235: well = floor(x/L), cell = rint(x/L) (ties to even),
+// local barrier = (xp < xc) ? 0 : 1.
+template <bool DBL>
+__device__ __forceinline__ void indices(const KConst& k, T64& t) {
+    const double red = t.x * k.invL;
+    t.well = (int64_t)floor(red);
+    t.cell = (int64_t)rint(red);
+    if (DBL) {
+        const double xp = t.x - (double)t.cell * k.L;
+        t.lb = (xp < k.xc) ? 0 : 1;
+    } else {
+        t.lb = 0;
+    }
+}
+
+template <bool DBL>
+__device__ __forceinline__ int table_state(const KConst& k, const TrajState& st, int64_t i, uint32_t g,
+                                           int64_t cell) {
+    int s;
+    int64_t stamp;
+    ring_load<DBL>(k, st, i, g, cell_key<DBL>(cell, 0), &s, &stamp);
+    return s;
+}
+
+// Initial-barrier bookkeeping of the FPT statistic, S.h:2187-2211 and
+// S.h:2364-2388; the two recorded states live in bits B_INIT0/B_INIT1.
+template <bool DBL>
+__device__ __forceinline__ void fpt_set_initial(const KConst& k, const TrajState& st, int64_t i, uint32_t g,
+                                                T64& t) {
+    int s0, s1;
+    if (t.well == t.cell) {
+        s0 = t.state;
+        t.init_idx0 = t.cell;
+        s1 = table_state<DBL>(k, st, i, g, t.cell + 1);
+        t.init_idx1 = t.cell + 1;
+    } else {
+        s0 = table_state<DBL>(k, st, i, g, t.cell - 1);
+        t.init_idx0 = t.cell - 1;
+        s1 = t.state;
+        t.init_idx1 = t.cell;
+    }
+    t.bits = (t.bits & ~(B_INIT0 | B_INIT1)) | (s0 ? B_INIT0 : 0u) | (s1 ? B_INIT1 : 0u);
+}
+
+__device__ __forceinline__ void fpt2_set_idx(T64& t) {
+    if (t.well == t.cell) { t.idx2_0 = t.cell; t.idx2_1 = t.cell + 1; }
+    else { t.idx2_0 = t.cell - 1; t.idx2_1 = t.cell; }
+}
+
+__device__ __forceinline__ bool cg_hit(int64_t well, int size) { return ((int)well % size) == 0; }
+
+__device__ __forceinline__ void record(const KConst& k, const TrajState& st, const T64& t, int64_t i,
+                                       int64_t frame) {
+    const int64_t o = frame * st.n + i;
+    if (st.fx) st.fx[o] = t.x;
+    if (k.write_x) {
+        if (st.fv) st.fv[o] = t.v;
+        if (st.ff) st.ff[o] = t.F;
+        if (st.fb) st.fb[o] = t.barrier;
+        if (st.fpe) st.fpe[o] = t.E;
+        if (st.fke) st.fke[o] = k.mhalf * (t.v * t.v);
+        if (st.fst) st.fst[o] = (double)t.state;
+    }
+}
+
+__device__ __forceinline__ void store_traj(const TrajState& st, const T64& t, int64_t i) {
+    st.x[i] = t.x; st.v[i] = t.v; st.F[i] = t.F; st.rprev[i] = t.rprev;
+    st.cell[i] = t.cell; st.well[i] = t.well; st.state[i] = t.state; st.lb[i] = t.lb; st.bits[i] = (int32_t)t.bits;
+    st.fpt_last[i] = t.fpt_last; st.fpt2_last[i] = t.fpt2_last; st.tpt_last[i] = t.tpt_last;
+    st.tpt2_last[i] = t.tpt2_last;
+    st.init_idx0[i] = t.init_idx0; st.init_idx1[i] = t.init_idx1; st.idx2_0[i] = t.idx2_0; st.idx2_1[i] = t.idx2_1;
+    st.tpt2_well[i] = t.tpt2_well; st.wt_tick[i] = t.wt_tick;
+}
+
+__device__ __forceinline__ void load_traj(const TrajState& st, T64& t, int64_t i) {
+    t.x = st.x[i]; t.v = st.v[i]; t.F = st.F[i]; t.rprev = st.rprev[i];
+    t.cell = st.cell[i]; t.well = st.well[i]; t.state = st.state[i]; t.lb = st.lb[i]; t.bits = (uint32_t)st.bits[i];
+    t.fpt_last = st.fpt_last[i]; t.fpt2_last = st.fpt2_last[i]; t.tpt_last = st.tpt_last[i];
+    t.tpt2_last = st.tpt2_last[i];
+    t.init_idx0 = st.init_idx0[i]; t.init_idx1 = st.init_idx1[i]; t.idx2_0 = st.idx2_0[i]; t.idx2_1 = st.idx2_1[i];
+    t.tpt2_well = st.tpt2_well[i]; t.wt_tick = st.wt_tick[i];
+    t.E = 0.0; t.barrier = 0.0;
+}
+
+// IntegrateStep0 (S.h:1619-1652, overdamped S.h:2825-2832; D.h:1938-1971)
+// with InitializeBarrierState (S.h:1885-1915) and InitializeStatistics
+// (S.h:2166-2333, D.h:2759-2930).
+template <bool DBL, bool OVER>
+__global__ void __launch_bounds__(128) fp64_init_kernel(const KConst k, const TrajState st, int64_t g0) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.n) return;
+    const uint32_t g = (uint32_t)(g0 + i);
+    for (int s = 0; s < k.slots; ++s) {
+        st.ring_tag[(int64_t)s * st.n + i] = INT64_MIN;
+        st.ring_data[(int64_t)s * st.n + i] = 0;
+    }
+    for (int f = 0; f < LDP_NCOUNT; ++f) st.counts[(int64_t)f * st.n + i] = 0;
+    for (int f = 0; f < LDP_NSUM; ++f) st.sums[(int64_t)f * st.n + i] = 0.0;
+
+    T64 t;
+    t.x = k.x0;
+    t.v = 0.0; t.F = 0.0; t.E = 0.0; t.rprev = 0.0; t.barrier = 0.0;
+    t.bits = 0;
+    t.fpt_last = t.fpt2_last = t.tpt_last = t.tpt2_last = 0.0;
+    t.init_idx0 = t.init_idx1 = t.idx2_0 = t.idx2_1 = 0;
+    t.wt_tick = 0;
+    indices<DBL>(k, t);
+    const Words w0 = philox_at(0, g, TAG_INIT, k.key0, k.key1);
+    t.state = k.rs ? (((double)w0.w0 * 0x1p-32 <= k.p_first) ? 0 : 1) : k.init_state;
+    st.state0[i] = t.state;
+    st.counts[(int64_t)(t.state ? LDP_C_STATE1 : LDP_C_STATE0) * st.n + i] = 1;
+    double zv, zr;
+    gauss_pair_f64(w0.w1, w0.w2, &zv, &zr);
+    t.v = k.rv ? k.sig_v0 * zv : k.v0;
+    st.v0[i] = t.v;
+    energy_force<DBL>(k, t);
+    if (k.at_bottom) {
+        if (!DBL && k.fpt) fpt_set_initial<DBL>(k, st, i, g, t);
+        fpt2_set_idx(t);
+    } else {
+        t.bits |= B_FPT_UP | B_FPT2_UP;
+    }
+    if (!k.at_bottom) t.bits |= B_TPT_UP | B_TPT2_UP;
+    t.tpt2_well = t.well;
+    for (int j = 0; j < k.n_cg; ++j) {
+        st.cg_last[(int64_t)j * st.n + i] = 0.0;
+        st.cg_well[(int64_t)j * st.n + i] = t.well;
+        if (!(k.at_bottom && cg_hit(t.well, k.cg_size[j]))) t.bits |= (B_CG0 << j);
+    }
+    if (OVER) t.rprev = k.sig_r * zr;
+    if (!k.fp_mode) record(k, st, t, i, 0);
+    store_traj(st, t, i);
+}
+
+// Steps s_begin .. s_end-1 of the hot loop (Integrate, S.h:1403-1511):
+// IntegrateStepEta / IntegrateStep (S.h:1654-1706, 2833-2886; D.h:1973-2024,
+// 3448-3505) followed by UpdateStatistics (S.h:2334-2592, D.h:2931-3209).
+template <bool DBL, bool OVER, bool ETA>
+__global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const TrajState st, int64_t g0,
+                                                         uint64_t s_begin, uint64_t s_end) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.n) return;
+    const uint32_t g = (uint32_t)(g0 + i);
+    T64 t;
+    load_traj(st, t, i);
+    if (t.bits & B_DONE) return;
+    const int64_t n = st.n;
+    int64_t sc0 = st.counts[(int64_t)LDP_C_STATE0 * n + i];
+    int64_t sc1 = st.counts[(int64_t)LDP_C_STATE1 * n + i];
+    // Force at the current position (not stored between launches).
+    energy_force<DBL>(k, t);
+    uint32_t flags = 0;
+    uint64_t s = s_begin;
+    const uint64_t fs = k.freq_save;
+    for (; s < s_end; ++s) {
+        const uint64_t j = (s - 1) >> 1;
+        const bool odd = ((s - 1) & 1) != 0;
+        const Words w = philox_at(j, g, TAG_STEP, k.key0, k.key1);
+        double za, zb;
+        gauss_pair_f64(w.w0, w.w1, &za, &zb);
+        const double z = odd ? zb : za;
+        const uint32_t fw = odd ? w.w3 : w.w2;
+
+        const int64_t cell_prev = t.cell, well_prev = t.well;
+        const int lb_prev = t.lb;
+        if (OVER) {
+            const double rf = k.sig_r * z;
+            t.x = fma(t.F, k.c_drift, t.x);
+            t.x = t.x + rf;
+            t.x = t.x + t.rprev;
+            t.rprev = rf;
+        } else {
+            t.v = t.v + (k.invM * t.F) * k.hdt;
+            t.x = t.x + t.v * k.hdt;
+            t.v = k.expg * t.v + k.sig_v * z;
+            t.x = t.x + t.v * k.hdt;
+        }
+        if (!isfinite(t.x)) {
+            flags |= LDP_FLAG_NONFINITE;
+            t.bits |= B_DONE;
+            break;
+        }
+        indices<DBL>(k, t);
+        const bool dWell = t.well != well_prev;
+        const bool dCell = t.cell != cell_prev;
+        const bool dKey = DBL ? (t.lb != lb_prev) : dCell;
+
+        if (ETA) {
+            // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736.
+            const uint64_t T = k.eq ? k.T_eq : k.T_as[t.state];
+            const uint32_t Thi = (uint32_t)(T >> 32), Tlo = (uint32_t)T;
+            bool flip = fw < Thi;
+            if (fw == Thi) {
+                const Words wr = philox_at(s, g, TAG_REFINE, k.key0, k.key1);
+                flip = wr.w0 < Tlo;
+            }
+            if (flip) t.state ^= 1;
+            if (dKey) {
+                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, (int64_t)s);
+                int ps;
+                int64_t stamp;
+                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &stamp);
+                const double lap = (double)((int64_t)s - stamp);
+                const double pl = k.c_lap[k.eq ? 0 : ps] * -expm1_f64(k.a_lap * lap);
+                const uint64_t Tl = prob_to_u64(pl);
+                const Words wc = philox_at(s, g, TAG_CATCHUP, k.key0, k.key1);
+                const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
+                t.state = (U < Tl) ? (ps ^ 1) : ps;
+            }
+        } else {
+            // UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434.
+            if (dKey) {
+                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, (int64_t)s);
+                int ps;
+                int64_t stamp;
+                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &stamp);
+                t.state = ps;
+            }
+        }
+        if (t.state) ++sc1; else ++sc0;   // UpdateBarrierStateEtaParamter
+        energy_force<DBL>(k, t);
+        if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+
+        // UpdateStatistics.
+        if (dWell || dCell) {
+            const double now = k.dt * (double)s;
+            if (!DBL && k.wt && !k.fp_mode) {
+                if (dWell) { t.wt_tick = (int64_t)s; t.bits |= B_WT_PASSED; }
+                else if (dCell && (t.bits & B_WT_PASSED)) {
+                    int64_t& nwt = st.counts[(int64_t)LDP_C_WT * n + i];
+                    if (nwt < k.tick_cap) st.ticks[i * k.tick_cap + nwt] = t.wt_tick;
+                    else flags |= LDP_FLAG_TICK_OVERFLOW;
+                    nwt += 1;
+                    t.bits &= ~B_WT_PASSED;
+                }
+            }
+            if (k.fpt || k.fp_mode) {
+                if (!DBL && !k.fp_mode) {
+                    if ((t.bits & B_FPT_UP) && dCell) {
+                        t.bits &= ~B_FPT_UP;
+                        t.fpt_last = now;
+                        fpt_set_initial<DBL>(k, st, i, g, t);
+                    }
+                    if (!(t.bits & B_FPT_UP) && dWell) {
+                        t.bits |= B_FPT_UP;
+                        st.sums[(int64_t)LDP_S_FPT * n + i] += now - t.fpt_last;
+                        st.counts[(int64_t)LDP_C_FPT * n + i] += 1;
+                        const bool ib = ((double)t.cell == (double)t.init_idx0) ? ((t.bits & B_INIT0) != 0)
+                                                                                : ((t.bits & B_INIT1) != 0);
+                        st.counts[(int64_t)(ib ? LDP_C_INIT1 : LDP_C_INIT0) * n + i] += 1;
+                        st.counts[(int64_t)(t.state ? LDP_C_INST1 : LDP_C_INST0) * n + i] += 1;
+                    }
+                }
+                if ((t.bits & B_FPT2_UP) && dCell) {
+                    t.bits &= ~B_FPT2_UP;
+                    t.fpt2_last = now;
+                    fpt2_set_idx(t);
+                }
+                if (dCell && !(t.bits & B_FPT2_UP) && t.idx2_0 != t.cell && t.idx2_1 != t.cell) {
+                    st.sums[(int64_t)LDP_S_FPT2 * n + i] += now - t.fpt2_last;
+                    st.counts[(int64_t)LDP_C_FPT2 * n + i] += 1;
+                    t.fpt2_last = now;
+                    fpt2_set_idx(t);
+                    if (k.fp_mode) t.bits |= B_DONE;   // first passage reached
+                }
+            }
+            if (!DBL && k.tpt && !k.fp_mode) {
+                if (dCell) { t.bits &= ~B_TPT_UP; t.tpt_last = now; }
+                if (!(t.bits & B_TPT_UP) && dWell) {
+                    t.bits |= B_TPT_UP;
+                    st.sums[(int64_t)LDP_S_TPT * n + i] += now - t.tpt_last;
+                    st.counts[(int64_t)LDP_C_TPT * n + i] += 1;
+                }
+                if (dCell) {
+                    if (t.bits & B_TPT2_UP) t.bits &= ~B_TPT2_UP;
+                    else if (t.well != t.tpt2_well) {
+                        st.sums[(int64_t)LDP_S_TPT2 * n + i] += now - t.tpt2_last;
+                        st.counts[(int64_t)LDP_C_TPT2 * n + i] += 1;
+                    }
+                    t.tpt2_last = now;
+                    t.tpt2_well = t.well;
+                }
+            }
+            if (k.cg && !k.fp_mode && dCell) {
+                for (int jj = 0; jj < k.n_cg; ++jj) {
+                    if (cg_hit(t.well, k.cg_size[jj])) {
+                        const int64_t o = (int64_t)jj * n + i;
+                        if (t.bits & (B_CG0 << jj)) {
+                            t.bits &= ~(B_CG0 << jj);
+                            st.cg_last[o] = now;
+                            st.cg_well[o] = t.well;
+                        } else if (t.well != st.cg_well[o]) {
+                            st.sums[(int64_t)(LDP_S_CG0 + jj) * n + i] += now - st.cg_last[o];
+                            st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i] += 1;
+                            st.cg_last[o] = now;
+                            st.cg_well[o] = t.well;
+                        }
+                    }
+                }
+            }
+        }
+        if (!k.fp_mode && (s % fs) == 0) record(k, st, t, i, (int64_t)(s / fs));
+        if (t.bits & B_DONE) { ++s; break; }
+    }
+    // s is the first step not integrated.
+    st.counts[(int64_t)LDP_C_STATE0 * n + i] = sc0;
+    st.counts[(int64_t)LDP_C_STATE1 * n + i] = sc1;
+    st.counts[(int64_t)LDP_C_STEPS * n + i] = (int64_t)s - 1;
+    if (k.fp_mode && !(t.bits & B_DONE) && s_end > k.step_cap) flags |= LDP_FLAG_CENSORED;
+    if (flags) st.counts[(int64_t)LDP_C_FLAGS * n + i] |= (int64_t)flags;
+    store_traj(st, t, i);
+}
+
+template <bool DBL, bool OVER>
+static int launch_init_t(const KConst& k, const TrajState& st, int64_t g0, int block, cudaStream_t stream) {
+    const int64_t grid = (st.n + block - 1) / block;
+    fp64_init_kernel<DBL, OVER><<<(unsigned)grid, block, 0, stream>>>(k, st, g0);
+    return (int)cudaGetLastError();
+}
+
+int launch_fp64_init(const KConst& k, const TrajState& st, int64_t g0, int block, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    block = 128;
+    if (k.dbl) return k.over ? launch_init_t<true, true>(k, st, g0, block, s) : launch_init_t<true, false>(k, st, g0, block, s);
+    return k.over ? launch_init_t<false, true>(k, st, g0, block, s) : launch_init_t<false, false>(k, st, g0, block, s);
+}
+
+template <bool DBL, bool OVER, bool ETA>
+static int launch_steps_t(const KConst& k, const TrajState& st, int64_t g0, uint64_t s0, uint64_t s1, int block,
+                          cudaStream_t stream) {
+    const int64_t grid = (st.n + block - 1) / block;
+    fp64_steps_kernel<DBL, OVER, ETA><<<(unsigned)grid, block, 0, stream>>>(k, st, g0, s0, s1);
+    return (int)cudaGetLastError();
+}
+
+int launch_fp64_steps(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end, int block,
+                      void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    block = 128;
+    const int sel = (k.dbl ? 4 : 0) | (k.over ? 2 : 0) | (k.eta ? 1 : 0);
+    switch (sel) {
+        case 0: return launch_steps_t<false, false, false>(k, st, g0, s_begin, s_end, block, s);
+        case 1: return launch_steps_t<false, false, true>(k, st, g0, s_begin, s_end, block, s);
+        case 2: return launch_steps_t<false, true, false>(k, st, g0, s_begin, s_end, block, s);
+        case 3: return launch_steps_t<false, true, true>(k, st, g0, s_begin, s_end, block, s);
+        case 4: return launch_steps_t<true, false, false>(k, st, g0, s_begin, s_end, block, s);
+        case 5: return launch_steps_t<true, false, true>(k, st, g0, s_begin, s_end, block, s);
+        case 6: return launch_steps_t<true, true, false>(k, st, g0, s_begin, s_end, block, s);
+        default: return launch_steps_t<true, true, true>(k, st, g0, s_begin, s_end, block, s);
+    }
+}
+
+}  // namespace ldp

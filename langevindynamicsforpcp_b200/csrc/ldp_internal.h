@@ -1,0 +1,76 @@
+// ldp_internal.h -- library-private definitions of the opaque C ABI handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ldp_engine.h"
+
+namespace ldp {
+struct Fp32Runtime;
+}
+
+constexpr int kCtxMarks = 16;
+
+struct ldp_ctx {
+    cudaEvent_t marks[kCtxMarks] = {};   // ldp_ctx_mark / ldp_ctx_elapsed_ms
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    std::mutex mu;
+    std::string err;
+    // FP32 batched path: runtime (queues, slots) and its launch shape.
+    ldp::Fp32Runtime* fp32 = nullptr;
+    int fp32_block = 0;            // threads per block (0: default 256)
+    int fp32_blocks_per_sm = 0;    // resident blocks per SM (0: default 4)
+    uint64_t fp32_pair_budget = 0; // step pairs per slot per launch (0: default)
+    int fp32_ring_slots = 0;       // cell-table ring slots per slot (0: default 64)
+};
+
+struct ldp_job {
+    ldp_ctx* ctx = nullptr;
+    ldp_params p{};
+    ldp_job_opts o{};
+    ldp::KConst k{};
+    int64_t ntraj = 0;
+    int64_t nframe = 0;
+    uint64_t nsteps = 0;
+    uint32_t seed = 0;
+    std::vector<int64_t> lags;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    ldp::TrajState st{};
+    double* d_msd0 = nullptr;
+    double* d_msd = nullptr;
+    int64_t* d_lags = nullptr;
+    void* d_aux = nullptr;   // 4 KiB of job-private device scratch
+    int64_t* d_ssum = nullptr;   // FP32 batched: event durations in steps [LDP_NSUM][ntraj]
+    int32_t* d_i32b = nullptr;   // FP32 batched: 32-bit statistics state
+    int fp32_type = -1;          // FP32 batched: queue (dbl*2 + over) the job is in
+    int fp32_slot = -1;          // FP32 batched: index in that queue's job table
+    bool finalized = false;      // results post-processed after completion
+    int fp32_phase = 0;          // 0 idle, 1 integrating, 2 finalizing
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool submitted = false;
+    bool done = false;
+    int64_t launches = 0;
+    int64_t steps_total = 0;
+    double wall_start = 0.0;
+    int64_t particle_steps_done() const;
+};
+
+void ldp_set_error(ldp_ctx* ctx, const char* fmt, ...);
+
+namespace ldp {
+int fp32_register(ldp_job* job);
+int fp32_pump(ldp_job* job, int nlaunch);
+int fp32_estimate_launches(const ldp_job* job);
+int fp32_remaining(ldp_job* job, unsigned long long* rem);
+int fp32_finalize(ldp_job* job);
+void fp32_release(ldp_job* job);
+void fp32_destroy_runtime(ldp_ctx* ctx);
+}  // namespace ldp
+std::vector<int64_t> ldp_lag_grid(const ldp_params& p);

@@ -1,0 +1,159 @@
+"""FP32 batched persistent path.
+
+* Deterministic: results do not depend on the launch shape (slots, blocks,
+  step budget per launch) nor on which other jobs share the batch -- every
+  random draw is keyed by (seed, job, trajectory, step).
+* Accurate: its statistics agree with the FP64 device path (which is
+  bit-identical to the CPU oracle) within the tolerances stated per test;
+  both paths integrate the same Philox noise, so the comparison is tight.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import langevindynamicsforpcp_b200 as ldp
+from langevindynamicsforpcp_b200 import _lib as L
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "inp")
+pytestmark = pytest.mark.gpu
+
+
+def quick(steps=120_000, freq=40, **kw):
+    p = ldp.params_from_inp(os.path.join(GOLDEN, "quick_test__2.0_7.2_m1.0_1.00e-05.inp"))
+    p.number_of_steps, p.freq_save, p.random_seed = steps, freq, 1234
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def double(steps=120_000, freq=40, **kw):
+    p = ldp.params_from_inp(os.path.join(GOLDEN, "CuIDB_double__2.0_7.2_m1.0_1.00e-05.inp"), ldp.MODEL_DOUBLE)
+    p.number_of_steps, p.freq_save, p.random_seed = steps, freq, 1234
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def run(ctx, p, precision, **kw):
+    with ldp.Job(ctx, p, precision=precision, **kw) as job:
+        job.run()
+        r = job.results()
+        if kw.get("mode", 0) == 0:
+            r["lags"], r["msd"] = job.msd()
+        r["timing"] = job.timing()
+    return r
+
+
+def same(a, b):
+    for k in ("counts", "sums", "state0", "v0", "x_final", "v_final", "state_final"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    for k in a:
+        if k.startswith("frames_") or k in ("ticks", "msd"):
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+@pytest.fixture(scope="module")
+def shapes():
+    # Two contexts with different persistent launch shapes.
+    a = ldp.Context(0)
+    b = ldp.Context(0)
+    L.lib()  # loaded
+    import ctypes as C  # noqa: F401
+    yield a, b
+    a.close()
+    b.close()
+
+
+def set_shape(ctx, block, bps, budget, ring=64):
+    # The launch shape lives in the context (set before first FP32 use).
+    from langevindynamicsforpcp_b200 import _tune
+    _tune.set_fp32_shape(ctx, block=block, blocks_per_sm=bps, pair_budget=budget, ring_slots=ring)
+
+
+def test_fp32_results_independent_of_launch_shape():
+    p = quick(write_x=1)
+    with ldp.Context(0) as c1, ldp.Context(0) as c2:
+        set_shape(c1, 256, 0, 1 << 15)
+        set_shape(c2, 128, 1, 777)      # tiny budget: many launches, many refills
+        a = run(c1, p, ldp.PREC_FP32_BATCHED, lanes=64, ranks=4)
+        b = run(c2, p, ldp.PREC_FP32_BATCHED, lanes=64, ranks=4)
+    same(a, b)
+    assert a["counts"][L.C_STEPS].min() == 120_000
+
+
+def test_fp32_double_and_underdamped_independent_of_launch_shape():
+    for p in (double(), quick(overdamped=0), double(overdamped=0)):
+        with ldp.Context(0) as c1, ldp.Context(0) as c2:
+            set_shape(c1, 256, 0, 1 << 15)
+            set_shape(c2, 64, 2, 333)
+            a = run(c1, p, ldp.PREC_FP32_BATCHED, lanes=128)
+            b = run(c2, p, ldp.PREC_FP32_BATCHED, lanes=128)
+        same(a, b)
+
+
+def test_fp32_job_results_same_alone_and_in_a_shared_batch(ctx):
+    pa = quick(steps=60_000, freq=20)
+    pb = quick(steps=200_000, freq=50, tau=1e-3)
+    alone = run(ctx, pa, ldp.PREC_FP32_BATCHED, lanes=256, job_id=7)
+    with ldp.Job(ctx, pb, precision=ldp.PREC_FP32_BATCHED, lanes=512, job_id=8) as jb, \
+            ldp.Job(ctx, pa, precision=ldp.PREC_FP32_BATCHED, lanes=256, job_id=7) as ja:
+        jb.submit()
+        ja.submit()
+        ja.wait()
+        jb.wait()
+        mixed = ja.results()
+        mixed["lags"], mixed["msd"] = ja.msd()
+    same(alone, mixed)
+
+
+def test_fp32_first_passage_refill_independent_of_shape():
+    p = quick()
+    with ldp.Context(0) as c1, ldp.Context(0) as c2:
+        set_shape(c1, 256, 0, 1 << 14)
+        set_shape(c2, 32, 1, 100)
+        a = run(c1, p, ldp.PREC_FP32_BATCHED, lanes=2048, mode=1, step_cap=2_000_000)
+        b = run(c2, p, ldp.PREC_FP32_BATCHED, lanes=2048, mode=1, step_cap=2_000_000)
+    same(a, b)
+    c = a["counts"]
+    assert np.all((c[L.C_FPT2] == 1) ^ ((c[L.C_FLAGS] & L.FLAG_CENSORED) != 0))
+
+
+def pooled(r, ci, si):
+    c = r["counts"][ci].sum()
+    return r["sums"][si].sum() / max(c, 1), c
+
+
+def test_fp32_statistics_agree_with_fp64(ctx):
+    # 4096 trajectories x 4e5 steps of the quick_test model (dt 1e-4).
+    # Tolerances: pooled MFPT / MFPT2 / MTPT within 1.5%, state fractions
+    # within 1e-3, MSD within 2% at every lag with more than 100 origins.
+    p = quick(steps=400_000, freq=100)
+    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=4096)
+    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=4096)
+    for ci, si in ((L.C_FPT, L.S_FPT), (L.C_FPT2, L.S_FPT2), (L.C_TPT, L.S_TPT)):
+        ma, na = pooled(a, ci, si)
+        mb, nb = pooled(b, ci, si)
+        assert na > 1000 and nb > 1000
+        assert abs(mb - ma) / ma < 0.015, (ci, ma, mb)
+    fa = a["counts"][L.C_STATE1].sum() / (a["counts"][L.C_STATE0].sum() + a["counts"][L.C_STATE1].sum())
+    fb = b["counts"][L.C_STATE1].sum() / (b["counts"][L.C_STATE0].sum() + b["counts"][L.C_STATE1].sum())
+    assert abs(fa - fb) < 1e-3
+    nf = p.number_of_steps // p.freq_save + 1
+    ok = (nf - a["lags"]) > 100
+    ok[0] = False
+    np.testing.assert_allclose(b["msd"][ok], a["msd"][ok], rtol=0.02)
+
+
+def test_fp32_first_passage_times_track_fp64(ctx):
+    # Same noise words: most trajectories reach their first passage on the
+    # same step in both precisions; the mean differs by well under 1%.
+    p = quick()
+    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=4096, mode=1, step_cap=3_000_000)
+    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=4096, mode=1, step_cap=3_000_000)
+    ta, tb = a["sums"][L.S_FPT2], b["sums"][L.S_FPT2]
+    ok = (a["counts"][L.C_FPT2] == 1) & (b["counts"][L.C_FPT2] == 1)
+    assert ok.mean() > 0.99
+    same_step = np.isclose(ta[ok], tb[ok], rtol=0, atol=0.5 * p.timestep)
+    assert same_step.mean() > 0.5, same_step.mean()
+    assert abs(tb[ok].mean() - ta[ok].mean()) / ta[ok].mean() < 0.01
