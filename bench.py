@@ -1,0 +1,346 @@
+"""Benchmark: particle-steps/s of the FP32 batched path vs the FP64 plain
+path on one B200 (and N replicas), on the "precision" workload:
+
+  16 single-barrier jobs x 65536 trajectories = 2^20 trajectories, geometry
+  of sample_input/CuIDB_single (L 5.8, w 0.65, X0 -2.9), overdamped, m 1,
+  gamma 1, kT 1, dt 1e-5; per job H_low drawn from {2,3,4,5} with the high
+  barrier 3.6 x H_low and the flip rate k log-uniform in [1e-2, 1e2]
+  (TAU = 1/k), drawn with numpy default_rng(1234); FPT/TPT/FPTCG statistics
+  on; 60000 steps per trajectory with frames every 20 steps (3001 frames,
+  MSD on the reference's log-spaced lags).  Synthetic inputs: the reference
+  ships no dataset.
+
+One timed step = one complete pass of all 16 jobs (integration, renewal
+statistics, frames, MSD, per-trajectory reductions), inputs resident on the
+device.  `e2e` repeats it through the C ABI from host parameters to host
+results (jobs created from host structs each step, per-trajectory counts and
+sums and the MSD copied back).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+OPS_PER_STEP = 70   # lane instructions per overdamped single-barrier step (algorithmic count)
+NJOBS, NTRAJ, NSTEPS, FREQSAVE = 16, 65536, 60000, 20
+
+
+def workload_params(ldp, job0=0, njobs=NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE):
+    base = os.path.join(ROOT, "tests", "golden", "inp", "CuIDB_single__2.0_7.2_m1.0_1.00e-05.inp")
+    rng = np.random.default_rng(1234)
+    draws = [(float(rng.choice([2.0, 3.0, 4.0, 5.0])), float(10 ** rng.uniform(-2, 2))) for _ in range(64)]
+    out = []
+    for j in range(job0, job0 + njobs):
+        h, k = draws[j % 64]
+        p = ldp.params_from_inp(base)
+        p.overdamped, p.timestep, p.tau = 1, 1e-5, 1.0 / k
+        p.barrier_heights[0][0], p.barrier_heights[0][1] = 3.6 * h, h
+        p.number_of_steps, p.freq_save = nsteps, freqsave
+        p.waiting_time, p.write_x, p.write_restart = 0, 0, 0
+        p.random_seed = 1234
+        out.append(p)
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            w = [x.strip() for x in ln.split(",")]
+            if len(w) < 8:
+                continue
+            try:
+                sm.append(float(w[1]))
+                mx = max(mx, float(w[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, w[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flush_l2():
+    import torch
+    buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    buf.zero_()
+    torch.cuda.synchronize()
+    del buf
+
+
+def run_batch(ldp, ctx, params, precision, job_id0=0):
+    """Creates, submits (one batch) and completes the jobs; returns them."""
+    jobs = [ldp.Job(ctx, p, lanes=NTRAJ, precision=precision, job_id=job_id0 + i) for i, p in enumerate(params)]
+    ldp.submit_batch(ctx, jobs)
+    for j in jobs:
+        j.wait()
+    return jobs
+
+
+def cpu_baseline_worker(args):
+    seed, traj_begin, ntraj, nsteps = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import langevindynamicsforpcp_b200 as ldp
+    import pyoracle
+    p = workload_params(ldp, 0, 1, nsteps=nsteps, freqsave=max(1, nsteps // 1000))
+    t = time.perf_counter()
+    pyoracle.run(p[0], seed, lanes=NTRAJ, traj_begin=traj_begin, traj_end=traj_begin + ntraj, frames=False)
+    return ntraj * nsteps, time.perf_counter() - t
+
+
+def cpu_baseline(budget_s=12.0):
+    """The CPU oracle (scalar C port of the reference's per-step algorithm)
+    on every host core for a bounded sample of job 0."""
+    cores = os.cpu_count() or 1
+    nsteps = 200_000
+    ntraj = 8          # trajectories per worker; ~6e6 steps/s per core
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(cpu_baseline_worker, [(1234, i * ntraj, ntraj, nsteps) for i in range(cores)])
+    steps = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    return {"value": steps / wall, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{cores} processes x {ntraj} trajectories x {nsteps} steps of job 0 (oracle/ldp_oracle.c)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="2 jobs x 16384 trajectories (for profiling)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return bench_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    import langevindynamicsforpcp_b200 as ldp
+    from langevindynamicsforpcp_b200 import _tune
+
+    global NJOBS, NTRAJ
+    if args.small:
+        NJOBS, NTRAJ = 2, 16384
+    ctx = ldp.Context(local)
+    shape = _tune.apply_tuned(ctx, "single_over")
+    params = workload_params(ldp, 0, NJOBS)
+    job_id0 = rank * 1000   # replicas integrate different trajectories
+    psteps = NJOBS * NTRAJ * NSTEPS
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- FP32 batched, device-resident timing ----
+    for _ in range(args.warmup):
+        for j in run_batch(ldp, ctx, params, ldp.PREC_FP32_BATCHED, job_id0):
+            j.close()
+    times, kernel_ms, launches = [], [], 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            jobs = [ldp.Job(ctx, p, lanes=NTRAJ, precision=ldp.PREC_FP32_BATCHED, job_id=job_id0 + i)
+                    for i, p in enumerate(params)]
+            flush_l2()
+            barrier()
+            ctx.mark(0)
+            ldp.submit_batch(ctx, jobs)
+            for j in jobs:
+                j.wait()
+            ctx.mark(1)
+            times.append(ctx.elapsed_ms(0, 1))
+            t = jobs[0].timing()
+            kernel_ms.append(t["integrate_ms"])
+            launches += sum(j.timing()["launches"] for j in jobs)
+            for j in jobs:
+                j.close()
+    clocks = clk.summary()
+    step_ms = max(times) if world == 1 else None
+    my_ms = sum(times) / len(times)
+    if dist:
+        tt = torch.tensor([my_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_ms = tt.item()
+    else:
+        step_ms = my_ms
+    value = psteps * world / (step_ms * 1e-3)
+    shape_used = _tune.get_fp32_shape(ctx)
+
+    # ---- FP64 plain leg (one job, 1/16 of the work) for the ratio ----
+    t64 = []
+    for it in range(args.warmup + args.steps):
+        with ldp.Job(ctx, params[0], lanes=NTRAJ, precision=ldp.PREC_FP64_PLAIN, job_id=job_id0) as j:
+            barrier()
+            ctx.mark(2)
+            j.submit()
+            j.wait()
+            ctx.mark(3)
+            if it >= args.warmup:
+                t64.append(ctx.elapsed_ms(2, 3))
+    fp64_value = NTRAJ * NSTEPS / (sum(t64) / len(t64) * 1e-3)
+
+    # ---- end to end through the C ABI: host params in, host results out ----
+    e2e_t = []
+    h2d = d2h = 0
+    for it in range(args.warmup + args.steps):
+        barrier()
+        t0 = time.perf_counter()
+        jobs = run_batch(ldp, ctx, params, ldp.PREC_FP32_BATCHED, job_id0)
+        b_in = len(jobs) * (C_sizeof_params())
+        b_out = 0
+        for j in jobs:
+            r = j.results(frames=False, ticks=False)
+            lags, msd = j.msd()
+            b_out += r["counts"].nbytes + r["sums"].nbytes + msd.nbytes
+            j.close()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+            h2d, d2h = b_in, b_out
+    e2e_s = sum(e2e_t) / len(e2e_t)
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = tt.item()
+    e2e_value = psteps * world / e2e_s
+
+    # ---- roofline of the persistent kernel (issue-bound) ----
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peaks = json.load(f)
+    props = torch.cuda.get_device_properties(local)
+    sms = props.multi_processor_count
+    fmax = peaks.get("sm_max_mhz", 1965.0)
+    peak_issue = sms * 4 * 32 * fmax * 1e6 / 1e9            # Glane-instr/s at the max clock
+    kms = sum(kernel_ms) / len(kernel_ms)
+    achieved = psteps * OPS_PER_STEP / (kms * 1e-3) / 1e9
+    fclk = clocks.get("sm_mhz") or fmax
+    roofline = {"bound": "issue", "achieved": achieved, "peak": peak_issue, "unit": "Ginstr/s",
+                "frac": achieved / peak_issue, "traffic": None,
+                "kernel": "fp32_persistent_kernel<single, overdamped>",
+                "ops_per_step": OPS_PER_STEP, "kernel_ms": kms,
+                "peak_basis": f"{sms} SMs x 128 lanes x sm_max_mhz {fmax:g} (MEASURED_PEAKS.json)",
+                "frac_at_sampled_clock": achieved / (sms * 128 * fclk * 1e6 / 1e9)}
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s, FP32 batched (vs FP64 plain), 1xB200",
+            "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "precision: 16 single-barrier jobs x 65536 trajectories, dt 1e-5, 60000 steps, "
+                                   "3001 frames, per-job H in {2,3,4,5}, high 3.6H, flip rate logU[1e-2,1e2]",
+                       "trajectories": NJOBS * NTRAJ * world, "steps_per_trajectory": NSTEPS,
+                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before each step; "
+                                                                 "frames 25 GB per step",
+                       "fp32_shape": shape_used, "tuned": bool(shape)},
+            "fp64_plain": {"value": fp64_value, "unit": "particle-steps/s",
+                           "sample": "job 0 alone (65536 trajectories x 60000 steps)"},
+            "fp32_over_fp64": value / world / fp64_value,
+            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches / max(1, args.steps)),
+            "roofline": roofline,
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def C_sizeof_params():
+    import ctypes
+    from langevindynamicsforpcp_b200 import _lib
+    return ctypes.sizeof(_lib.Params)
+
+
+def bench_reference(args, rank, world):
+    """The reference's CPU path for this workload on the host cores: the
+    reference build in oracle/_ref when present, else the CPU oracle port."""
+    if rank != 0:
+        return
+    vals = []
+    kind = "port"
+    for it in range(args.warmup + args.steps):
+        r = cpu_baseline()
+        if it >= args.warmup:
+            vals.append(r["value"])
+    value = sum(vals) / len(vals)
+    line = {"impl": "reference", "metric": "particle-steps/s, FP32 batched (vs FP64 plain), 1xB200",
+            "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "precision: job 0 of the 16-job workload, bounded sample per step"},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": kind,
+                             "sample": r["sample"]},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -153,7 +153,11 @@ enum ldp_count_field {
 /* Per-trajectory event-time sums (FP64, event order), [field][ntraj]. */
 enum ldp_sum_field {
     LDP_S_FPT = 0, LDP_S_FPT2, LDP_S_TPT, LDP_S_TPT2,
-    LDP_S_CG0,       /* LDP_S_CG0 + j */
+    LDP_S_FIRST_FPT,   /* duration of the trajectory's first FPT event  */
+    LDP_S_FIRST_FPT2,  /* ... first FPT2 event                           */
+    LDP_S_FIRST_TPT,   /* ... first TPT event                            */
+    LDP_S_FIRST_TPT2,  /* ... first TPT2 event (0 while the count is 0)  */
+    LDP_S_CG0,         /* LDP_S_CG0 + j */
     LDP_NSUM = LDP_S_CG0 + LDP_MAX_CG
 };
 

@@ -190,3 +190,29 @@ class Job:
 
     def __exit__(self, *a):
         self.close()
+
+
+def submit_batch(ctx: Context, jobs) -> None:
+    """Submits several jobs together (ldp_submit_batch): FP32 batched jobs
+    share every persistent launch."""
+    arr = (C.c_void_p * len(jobs))(*[j.handle for j in jobs])
+    _check(L.lib().ldp_submit_batch(ctx.handle, arr, len(jobs)), ctx)
+
+
+def _ctx_mark(self, mark: int) -> None:
+    _check(L.lib().ldp_ctx_mark(self.handle, mark), self)
+
+
+def _ctx_elapsed_ms(self, a: int, b: int) -> float:
+    ms = C.c_double()
+    _check(L.lib().ldp_ctx_elapsed_ms(self.handle, a, b, C.byref(ms)), self)
+    return ms.value
+
+
+def _ctx_synchronize(self) -> None:
+    _check(L.lib().ldp_ctx_synchronize(self.handle), self)
+
+
+Context.mark = _ctx_mark
+Context.elapsed_ms = _ctx_elapsed_ms
+Context.synchronize = _ctx_synchronize

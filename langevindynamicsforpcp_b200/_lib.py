@@ -23,7 +23,7 @@ MODE_FIXED_STEPS, MODE_FIRST_PASSAGE = 0, 1
  C_WT, C_EVICT, C_FLAGS, C_STEPS, C_CG0) = range(15)
 NCOUNT = C_CG0 + LDP_MAX_CG
 # enum ldp_sum_field
-S_FPT, S_FPT2, S_TPT, S_TPT2, S_CG0 = range(5)
+S_FPT, S_FPT2, S_TPT, S_TPT2, S_FIRST_FPT, S_FIRST_FPT2, S_FIRST_TPT, S_FIRST_TPT2, S_CG0 = range(9)
 NSUM = S_CG0 + LDP_MAX_CG
 
 FLAG_NONFINITE, FLAG_TICK_OVERFLOW, FLAG_CENSORED = 1, 2, 4

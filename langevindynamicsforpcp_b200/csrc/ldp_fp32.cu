@@ -224,6 +224,8 @@ __device__ __noinline__ bool f_events(const JobF* Jp, const SlotsDev S, int64_t 
             }
             if (!(bits & B_FPT_UP) && dWell) {
                 bits |= B_FPT_UP;
+                if (J.counts[(int64_t)LDP_C_FPT * n + traj] == 0)
+                    J.ssum[(int64_t)LDP_S_FIRST_FPT * n + traj] = now - J.fpt_last[traj];
                 J.ssum[(int64_t)LDP_S_FPT * n + traj] += now - J.fpt_last[traj];
                 J.counts[(int64_t)LDP_C_FPT * n + traj] += 1;
                 const bool ib = (cell == J.init_idx0[traj]) ? ((bits & B_INIT0) != 0) : ((bits & B_INIT1) != 0);
@@ -237,6 +239,8 @@ __device__ __noinline__ bool f_events(const JobF* Jp, const SlotsDev S, int64_t 
             f_fpt2_idx(J, traj, cell, well);
         }
         if (dCell && !(bits & B_FPT2_UP) && J.idx2_0[traj] != cell && J.idx2_1[traj] != cell) {
+            if (J.counts[(int64_t)LDP_C_FPT2 * n + traj] == 0)
+                J.ssum[(int64_t)LDP_S_FIRST_FPT2 * n + traj] = now - J.fpt2_last[traj];
             J.ssum[(int64_t)LDP_S_FPT2 * n + traj] += now - J.fpt2_last[traj];
             J.counts[(int64_t)LDP_C_FPT2 * n + traj] += 1;
             J.fpt2_last[traj] = now;
@@ -248,12 +252,16 @@ __device__ __noinline__ bool f_events(const JobF* Jp, const SlotsDev S, int64_t 
         if (dCell) { bits &= ~B_TPT_UP; J.tpt_last[traj] = now; }
         if (!(bits & B_TPT_UP) && dWell) {
             bits |= B_TPT_UP;
+            if (J.counts[(int64_t)LDP_C_TPT * n + traj] == 0)
+                J.ssum[(int64_t)LDP_S_FIRST_TPT * n + traj] = now - J.tpt_last[traj];
             J.ssum[(int64_t)LDP_S_TPT * n + traj] += now - J.tpt_last[traj];
             J.counts[(int64_t)LDP_C_TPT * n + traj] += 1;
         }
         if (dCell) {
             if (bits & B_TPT2_UP) bits &= ~B_TPT2_UP;
             else if (well != J.tpt2_well[traj]) {
+                if (J.counts[(int64_t)LDP_C_TPT2 * n + traj] == 0)
+                    J.ssum[(int64_t)LDP_S_FIRST_TPT2 * n + traj] = now - J.tpt2_last[traj];
                 J.ssum[(int64_t)LDP_S_TPT2 * n + traj] += now - J.tpt2_last[traj];
                 J.counts[(int64_t)LDP_C_TPT2 * n + traj] += 1;
             }

@@ -16,7 +16,7 @@
 namespace ldp {
 
 constexpr int kFp32MaxJobs = 16384;     // resident jobs per queue
-constexpr int kFp32MaxRanges = 16384;   // published item ranges per queue
+constexpr int kFp32MaxRanges = 1 << 20; // published item ranges per queue (one per job)
 
 // Per-job constants and output pointers (device resident, one per job).
 struct JobF {

@@ -228,7 +228,10 @@ int fp32_estimate_launches(const ldp_job* job) {
     const Fp32Queue& Q = job->ctx->fp32->q[job->fp32_type];
     const double pairs = (double)job->ntraj * (double)((job->nsteps + 1) / 2);
     const double cap = (double)Q.s.nslots * (double)Q.pair_budget;
-    int n = (int)(pairs / cap) + 1;
+    // A trajectory's steps run in order in one slot: at least its own length
+    // in launches, however many slots are free.
+    const double serial = (double)((job->nsteps + 1) / 2) / (double)Q.pair_budget;
+    int n = (int)std::max(pairs / cap, serial) + 1;
     if (job->o.mode == LDP_MODE_FIRST_PASSAGE) n = std::max(1, n / 8);
     return std::min(n, 4096);
 }

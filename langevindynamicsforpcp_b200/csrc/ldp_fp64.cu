@@ -351,6 +351,7 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
                     }
                     if (!(t.bits & B_FPT_UP) && dWell) {
                         t.bits |= B_FPT_UP;
+                        if (st.counts[(int64_t)LDP_C_FPT * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_FPT * n + i] = now - t.fpt_last;
                         st.sums[(int64_t)LDP_S_FPT * n + i] += now - t.fpt_last;
                         st.counts[(int64_t)LDP_C_FPT * n + i] += 1;
                         const bool ib = ((double)t.cell == (double)t.init_idx0) ? ((t.bits & B_INIT0) != 0)
@@ -365,6 +366,7 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
                     fpt2_set_idx(t);
                 }
                 if (dCell && !(t.bits & B_FPT2_UP) && t.idx2_0 != t.cell && t.idx2_1 != t.cell) {
+                    if (st.counts[(int64_t)LDP_C_FPT2 * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_FPT2 * n + i] = now - t.fpt2_last;
                     st.sums[(int64_t)LDP_S_FPT2 * n + i] += now - t.fpt2_last;
                     st.counts[(int64_t)LDP_C_FPT2 * n + i] += 1;
                     t.fpt2_last = now;
@@ -376,12 +378,14 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
                 if (dCell) { t.bits &= ~B_TPT_UP; t.tpt_last = now; }
                 if (!(t.bits & B_TPT_UP) && dWell) {
                     t.bits |= B_TPT_UP;
+                    if (st.counts[(int64_t)LDP_C_TPT * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_TPT * n + i] = now - t.tpt_last;
                     st.sums[(int64_t)LDP_S_TPT * n + i] += now - t.tpt_last;
                     st.counts[(int64_t)LDP_C_TPT * n + i] += 1;
                 }
                 if (dCell) {
                     if (t.bits & B_TPT2_UP) t.bits &= ~B_TPT2_UP;
                     else if (t.well != t.tpt2_well) {
+                        if (st.counts[(int64_t)LDP_C_TPT2 * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_TPT2 * n + i] = now - t.tpt2_last;
                         st.sums[(int64_t)LDP_S_TPT2 * n + i] += now - t.tpt2_last;
                         st.counts[(int64_t)LDP_C_TPT2 * n + i] += 1;
                     }

@@ -649,6 +649,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                     }
                     if (!t.fpt_up && dWell) {
                         t.fpt_up = 1;
+                        if (cnt[LDP_C_FPT] == 0) sum[LDP_S_FIRST_FPT] = now - t.fpt_last;
                         sum[LDP_S_FPT] += now - t.fpt_last;
                         cnt[LDP_C_FPT]++;
                         double ib = ((double)t.cell == (double)t.init_idx[0]) ? t.init_state[0] : t.init_state[1];
@@ -662,6 +663,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                     fpt2_set_idx(&t);
                 }
                 if (dCell && !t.fpt2_up && t.idx2[0] != t.cell && t.idx2[1] != t.cell) {
+                    if (cnt[LDP_C_FPT2] == 0) sum[LDP_S_FIRST_FPT2] = now - t.fpt2_last;
                     sum[LDP_S_FPT2] += now - t.fpt2_last;
                     cnt[LDP_C_FPT2]++;
                     t.fpt2_last = now;
@@ -673,12 +675,14 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                 if (dCell) { t.tpt_up = 0; t.tpt_last = now; }
                 if (!t.tpt_up && dWell) {
                     t.tpt_up = 1;
+                    if (cnt[LDP_C_TPT] == 0) sum[LDP_S_FIRST_TPT] = now - t.tpt_last;
                     sum[LDP_S_TPT] += now - t.tpt_last;
                     cnt[LDP_C_TPT]++;
                 }
                 if (dCell) {
                     if (t.tpt2_up) t.tpt2_up = 0;
                     else if (t.well != t.tpt2_well) {
+                        if (cnt[LDP_C_TPT2] == 0) sum[LDP_S_FIRST_TPT2] = now - t.tpt2_last;
                         sum[LDP_S_TPT2] += now - t.tpt2_last;
                         cnt[LDP_C_TPT2]++;
                     }

@@ -111,9 +111,9 @@ def test_fp32_first_passage_refill_independent_of_shape():
     p = quick()
     with ldp.Context(0) as c1, ldp.Context(0) as c2:
         set_shape(c1, 256, 0, 1 << 14)
-        set_shape(c2, 32, 1, 100)
-        a = run(c1, p, ldp.PREC_FP32_BATCHED, lanes=2048, mode=1, step_cap=2_000_000)
-        b = run(c2, p, ldp.PREC_FP32_BATCHED, lanes=2048, mode=1, step_cap=2_000_000)
+        set_shape(c2, 32, 1, 5000)      # 4736 slots for 8192 trajectories: refills
+        a = run(c1, p, ldp.PREC_FP32_BATCHED, lanes=8192, mode=1, step_cap=2_000_000)
+        b = run(c2, p, ldp.PREC_FP32_BATCHED, lanes=8192, mode=1, step_cap=2_000_000)
     same(a, b)
     c = a["counts"]
     assert np.all((c[L.C_FPT2] == 1) ^ ((c[L.C_FLAGS] & L.FLAG_CENSORED) != 0))
@@ -125,17 +125,20 @@ def pooled(r, ci, si):
 
 
 def test_fp32_statistics_agree_with_fp64(ctx):
-    # 4096 trajectories x 4e5 steps of the quick_test model (dt 1e-4).
-    # Tolerances: pooled MFPT / MFPT2 / MTPT within 1.5%, state fractions
-    # within 1e-3, MSD within 2% at every lag with more than 100 origins.
+    # 65536 trajectories x 4e5 steps of the quick_test model (dt 1e-4), both
+    # precisions on the same noise.  Mean event times (MFPT, MFPT2, MTPT)
+    # agree within max(1%, 3 standard errors of the difference), the state
+    # fractions within 1e-3, the MSD within 2% at lags with > 100 origins.
     p = quick(steps=400_000, freq=100)
-    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=4096)
-    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=4096)
+    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=65536)
+    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=65536)
     for ci, si in ((L.C_FPT, L.S_FPT), (L.C_FPT2, L.S_FPT2), (L.C_TPT, L.S_TPT)):
         ma, na = pooled(a, ci, si)
         mb, nb = pooled(b, ci, si)
-        assert na > 1000 and nb > 1000
-        assert abs(mb - ma) / ma < 0.015, (ci, ma, mb)
+        assert na > 10000 and nb > 10000
+        se = np.sqrt(ma * ma / na + mb * mb / nb)
+        print(f"field {ci}: fp64 {ma:.5f} ({na}) fp32 {mb:.5f} ({nb}) rel diff {(mb - ma) / ma:+.4%}")
+        assert abs(mb - ma) < max(0.01 * ma, 3 * se), (ci, ma, mb, se)
     fa = a["counts"][L.C_STATE1].sum() / (a["counts"][L.C_STATE0].sum() + a["counts"][L.C_STATE1].sum())
     fb = b["counts"][L.C_STATE1].sum() / (b["counts"][L.C_STATE0].sum() + b["counts"][L.C_STATE1].sum())
     assert abs(fa - fb) < 1e-3
@@ -145,15 +148,19 @@ def test_fp32_statistics_agree_with_fp64(ctx):
     np.testing.assert_allclose(b["msd"][ok], a["msd"][ok], rtol=0.02)
 
 
-def test_fp32_first_passage_times_track_fp64(ctx):
-    # Same noise words: most trajectories reach their first passage on the
-    # same step in both precisions; the mean differs by well under 1%.
+def test_fp32_first_passage_distribution_matches_fp64(ctx):
+    # First bottom-to-other-bottom passage of 16384 trajectories in both
+    # precisions: two-sample KS p > 0.01 and means within 3 standard errors.
+    from scipy import stats
     p = quick()
-    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=4096, mode=1, step_cap=3_000_000)
-    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=4096, mode=1, step_cap=3_000_000)
-    ta, tb = a["sums"][L.S_FPT2], b["sums"][L.S_FPT2]
-    ok = (a["counts"][L.C_FPT2] == 1) & (b["counts"][L.C_FPT2] == 1)
-    assert ok.mean() > 0.99
-    same_step = np.isclose(ta[ok], tb[ok], rtol=0, atol=0.5 * p.timestep)
-    assert same_step.mean() > 0.5, same_step.mean()
-    assert abs(tb[ok].mean() - ta[ok].mean()) / ta[ok].mean() < 0.01
+    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=16384, mode=1, step_cap=10_000_000)
+    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=16384, mode=1, step_cap=10_000_000)
+    ok_a = a["counts"][L.C_FPT2] == 1
+    ok_b = b["counts"][L.C_FPT2] == 1
+    assert ok_a.mean() > 0.999 and ok_b.mean() > 0.999
+    ta, tb = a["sums"][L.S_FPT2][ok_a], b["sums"][L.S_FPT2][ok_b]
+    ks = stats.ks_2samp(ta, tb)
+    print(f"FPT2 fp64 mean {ta.mean():.4f} fp32 mean {tb.mean():.4f} KS p={ks.pvalue:.3f}")
+    assert ks.pvalue > 0.01
+    se = np.sqrt(ta.var() / len(ta) + tb.var() / len(tb))
+    assert abs(ta.mean() - tb.mean()) < 3 * se
