@@ -279,6 +279,33 @@ ldp_status  ldp_job_msd_traj(ldp_job *job, double *msd0);
  * src/langevinDynamicsSingleBarrier.h:3594-4036. */
 ldp_status  ldp_job_write_outputs(ldp_job *job, const char *dir);
 
+/*
+ * FP64 plain integration that allocates nothing.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory -- a host
+ * application or framework that owns the whole device-memory budget, a
+ * real-time loop that cannot pay for an allocation (or the synchronization
+ * that freeing implies), a plugin that may only use the buffers it is given.
+ * The caller passes the parameters and its own device buffers for the
+ * outputs: d_counts [LDP_NCOUNT][ntraj], d_sums [LDP_NSUM][ntraj],
+ * d_x_final [ntraj], and optionally d_frames_x [nframe][ntraj] (NULL: no
+ * frames); ntraj = ranks * NUMBEROFRUNS * lanes, at most
+ * LDP_NOALLOC_MAX_TRAJ.  The working state lives in one fixed device array
+ * of the library (about 6 MB, held by every GPU that loads the library until
+ * the process exits); every call overwrites it, so calls whose device work
+ * overlaps (other streams, other host threads) race on it -- serialize them.
+ * The first call on a device looks up that array's address; make it before
+ * any stream capture.  The work is enqueued on `stream` (NULL: the current
+ * device's default stream) on the current device; the call returns without
+ * waiting.  Results equal ldp_job_create/ldp_submit with
+ * LDP_PREC_FP64_PLAIN for the same params and layout; RANDOMSEED < 0 means
+ * seed 0 here, WAITINGTIME and WRITEX series are not produced, fixed-step
+ * mode only.  Errors come back as a status and a message in err.
+ */
+#define LDP_NOALLOC_MAX_TRAJ 4096
+ldp_status  ldp_integrate_fp64_noalloc(const ldp_params *p, const ldp_job_opts *o, int64_t *d_counts,
+                                       double *d_sums, double *d_x_final, double *d_frames_x,
+                                       void *stream, char *err, size_t errlen);
+
 /* One-shot drop-in for `mpirun -n ranks ./exe -i path`. */
 ldp_status  ldp_run_inp(ldp_ctx *ctx, const char *path, int model,
                         const ldp_job_opts *o, const char *outdir);

@@ -27,6 +27,7 @@ S_FPT, S_FPT2, S_TPT, S_TPT2, S_FIRST_FPT, S_FIRST_FPT2, S_FIRST_TPT, S_FIRST_TP
 NSUM = S_CG0 + LDP_MAX_CG
 
 FLAG_NONFINITE, FLAG_TICK_OVERFLOW, FLAG_CENSORED = 1, 2, 4
+NOALLOC_MAX_TRAJ = 4096
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "device error", 4: "timeout",
           5: "i/o error", 6: "parse error", 7: "unsupported", 8: "not ready", 9: "restart error"}
@@ -127,6 +128,8 @@ SIGNATURES = {
     "ldp_job_msd_traj": (C.c_int, [C.c_void_p, _DP]),
     "ldp_job_write_outputs": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ldp_run_inp": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(JobOpts), C.c_char_p]),
+    "ldp_integrate_fp64_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(JobOpts), C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None
