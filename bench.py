@@ -159,6 +159,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="2 jobs x 16384 trajectories (for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nsteps", type=int, default=None, help="steps per trajectory (profiling cases)")
+    ap.add_argument("--njobs", type=int, default=None, help="jobs per batch (profiling cases)")
+    ap.add_argument("--ntraj", type=int, default=None, help="trajectories per job (profiling cases)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -179,12 +182,18 @@ def main():
     import langevindynamicsforpcp_b200 as ldp
     from langevindynamicsforpcp_b200 import _tune
 
-    global NJOBS, NTRAJ
+    global NJOBS, NTRAJ, NSTEPS
     if args.small:
         NJOBS, NTRAJ = 2, 16384
+    if args.nsteps:
+        NSTEPS = args.nsteps
+    if args.njobs:
+        NJOBS = args.njobs
+    if args.ntraj:
+        NTRAJ = args.ntraj
     ctx = ldp.Context(local)
     shape = _tune.apply_tuned(ctx, "single_over")
-    params = workload_params(ldp, 0, NJOBS)
+    params = workload_params(ldp, 0, NJOBS, nsteps=NSTEPS)
     job_id0 = rank * 1000   # replicas integrate different trajectories
     psteps = NJOBS * NTRAJ * NSTEPS
 
@@ -197,7 +206,7 @@ def main():
     for _ in range(args.warmup):
         for j in run_batch(ldp, ctx, params, ldp.PREC_FP32_BATCHED, job_id0):
             j.close()
-    times, kernel_ms, launches = [], [], 0
+    times, kernel_ms, msd_ms, launches = [], [], [], 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             jobs = [ldp.Job(ctx, p, lanes=NTRAJ, precision=ldp.PREC_FP32_BATCHED, job_id=job_id0 + i)
@@ -212,6 +221,7 @@ def main():
             times.append(ctx.elapsed_ms(0, 1))
             t = jobs[0].timing()
             kernel_ms.append(t["integrate_ms"])
+            msd_ms.append(sum(j.timing()["msd_ms"] for j in jobs))
             launches += sum(j.timing()["launches"] for j in jobs)
             for j in jobs:
                 j.close()
@@ -303,6 +313,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches / max(1, args.steps)),
+            "post_ms": sum(msd_ms) / len(msd_ms),
             "roofline": roofline,
             "clocks": clocks,
         }

@@ -6,19 +6,34 @@
 // the step in FP32:
 //  * position = cell * L + xp with an int cell index and an FP32 cell-local
 //    coordinate xp in [-L/2, L/2) (no FP32 absolute position);
-//  * Box-Muller noise on the special-function units (__logf, __sincosf) from
-//    the same Philox words the FP64 path uses, so both paths integrate the
-//    same noise sequence;
+//  * Box-Muller noise on the special-function units (lg2/sqrt/sin/cos
+//    approximations) from the same Philox words the FP64 path uses, the
+//    uniforms built from the words' high bits by exponent splicing;
 //  * an exact integer step counter as the clock; event durations are summed
 //    as integer step counts (exact), frames are saved as FP64 cell*L + xp.
-// The rare paths (cell entry catch-up, renewal statistics, frame records,
-// trajectory start/retire) are out-of-line functions so that the hot loop
-// keeps few registers.
+//
+// Hot loop.  The force of both models is piecewise constant in xp: between
+// consecutive "breakpoints" (cell edges, barrier flanks, the barrier top and,
+// for the double model, the flank meeting point) neither the force, the
+// cell, the well nor the local barrier changes.  Each thread keeps the open
+// band (lo, hi) around its position, the force of its current barrier state
+// and the high word of its flip threshold in registers, so a step is the
+// Philox/Box-Muller draw, the position update and three compares.  Every
+// step that leaves the band, draws a flip (or a threshold tie), or reaches a
+// frame or the last step takes the general step below, which follows the
+// FP64 step exactly (wrap, indices, flip, cell-table entry with lazy
+// catch-up, force, renewal statistics, frame, end).
+//
+// Rare state lives in shared memory (statistics clocks and flags, the cached
+// state of the cell left last, the state-1 step count), counts and duration
+// sums go out as fire-and-forget atomics, and the cell-table ring is written
+// through on every cell exit, so re-crossing back into the cell just left
+// needs no memory read.
 //
 // Batching: each thread is a slot that owns one trajectory; when it retires
 // (fixed step count reached, or first passage in FIRST_PASSAGE mode) the
-// warp's retired lanes claim new trajectories from the device work queue
-// with one compare-and-swap per warp and a ballot/popc prefix.
+// warp's idle lanes claim new trajectories from the device work queue with
+// one compare-and-swap per warp and a ballot/popc prefix.
 #include <cuda_runtime.h>
 
 #include "ldp_device.cuh"
@@ -30,9 +45,60 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kClaimTries = 1 << 16;   // bound of the claim retry loop
+constexpr int kMaxBlock = 256;
+constexpr int kLeftMax = 1 << 30;      // countdown clamp; a clamped zero is a no-op general step
 
-__device__ __forceinline__ int64_t fkey(bool dbl, int cell, int lb) {
-    return dbl ? (int64_t)cell * 2 + lb : (int64_t)cell;
+// Statistics flags used only by this path (bits 0..23 are the shared B_*).
+enum : uint32_t { B_HAS_FPT = 1u << 24, B_HAS_FPT2 = 1u << 25, B_HAS_TPT = 1u << 26, B_HAS_TPT2 = 1u << 27 };
+// Slot word: local barrier, eviction pending for the current cell, cache of
+// the cell left last (valid, its state).
+enum : int32_t { W_LB = 1, W_EVICT = 2, W_CVALID = 4, W_CSTATE = 8 };
+
+// Per-thread rare state, structure of arrays (conflict-free by thread).
+struct RareSm {
+    uint32_t bits[kMaxBlock];
+    int32_t init0[kMaxBlock];     // first cell of the FPT initial-barrier pair
+    int32_t idx2[kMaxBlock];      // first cell of the FPT2 reference pair
+    int32_t tpt2w[kMaxBlock];     // well of the last TPT2 renewal
+    int32_t ckey[kMaxBlock];      // key of the cell left last
+    int32_t cgw[kMaxBlock];       // well of the last FPTCG evaluation
+    int32_t fidx[kMaxBlock];      // index of the next frame
+    long long nxf[kMaxBlock];     // step of the next frame
+    long long fpt[kMaxBlock], fpt2[kMaxBlock], tpt[kMaxBlock], tpt2[kMaxBlock];
+    long long cstamp[kMaxBlock];  // step at which the cached cell was left
+    long long sc1[kMaxBlock];     // completed state-1 steps
+    long long since[kMaxBlock];   // first step of the current state-1 run
+};
+
+__device__ __forceinline__ void red_add(int64_t* p, int64_t v) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+
+__device__ __forceinline__ int fkey(bool dbl, int cell, int lb) { return dbl ? cell * 2 + lb : cell; }
+
+__device__ __forceinline__ uint32_t thi_of(const JobF& J, int st) {
+    return (uint32_t)((J.eq ? J.T_eq : J.T_as[st]) >> 32);
+}
+
+// Uniform in (0, 1): the high 23 bits of w as a mantissa, offset by 2^-24.
+__device__ __forceinline__ float unit_open(uint32_t w) {
+    return __int_as_float((int)__funnelshift_r(w, 0x7fu, 9)) - 0.99999994039535522461f;
+}
+// w * 2^-32 folded into [-1/2, 1/2) (same angle mod 1), 23 high bits.
+__device__ __forceinline__ float unit_centered(uint32_t w) {
+    return __int_as_float((int)(__funnelshift_r(w, 0x7fu, 9) ^ 0x00400000u)) - 1.5f;
+}
+
+// Box-Muller pair scaled by sigma: k = -2 ln 2 sigma^2 (log2 is the native
+// logarithm of the special-function unit).
+__device__ __forceinline__ void noise_pair(uint32_t wa, uint32_t wb, float k, float* n0, float* n1) {
+    const float t = fmaxf(__log2f(unit_open(wa)) * k, 0.0f);
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(t));
+    float sn, cs;
+    __sincosf(6.28318530717958647692f * unit_centered(wb), &sn, &cs);
+    *n0 = r * cs;
+    *n1 = r * sn;
 }
 
 __device__ int f_default_state(const JobF& J, bool dbl, uint32_t g, int64_t ck) {
@@ -48,86 +114,41 @@ __device__ int f_default_state(const JobF& J, bool dbl, uint32_t g, int64_t ck) 
     return ((double)w.w0 * 0x1p-32 < J.p_cell0) ? 0 : 1;
 }
 
-__device__ void f_ring_load(const JobF& J, const SlotsDev& S, int64_t slot, bool dbl, uint32_t g, int64_t ck,
-                            int* state, int64_t* stamp) {
-    const int64_t r = ck & (int64_t)(S.ring_slots - 1);
-    const int64_t o = r * S.nslots + slot;
-    if (S.ring_tag[o] == ck) {
-        const int64_t d = S.ring_data[o];
-        *state = (int)(d & 1);
-        *stamp = d >> 1;
-    } else {
-        *state = f_default_state(J, dbl, g, ck);
-        *stamp = 0;
-    }
+__device__ __forceinline__ int f_ring_state(const JobF& J, const SlotsDev& S, int64_t slot, bool dbl, uint32_t g,
+                                            int key) {
+    const longlong2 e = S.ring[(int64_t)(key & (S.ring_slots - 1)) * S.nslots + slot];
+    return (e.x == (long long)key) ? (int)(e.y & 1) : f_default_state(J, dbl, g, key);
 }
 
-__device__ void f_ring_store(const JobF& J, const SlotsDev& S, int64_t slot, int64_t traj, int64_t ck, int state,
-                             int64_t stamp) {
-    const int64_t r = ck & (int64_t)(S.ring_slots - 1);
-    const int64_t o = r * S.nslots + slot;
-    const int64_t old = S.ring_tag[o];
-    if (old != ck && old != INT64_MIN) J.counts[(int64_t)LDP_C_EVICT * J.ntraj + traj] += 1;
-    S.ring_tag[o] = ck;
-    S.ring_data[o] = (stamp << 1) | (int64_t)state;
-}
-
-// Cell (double model: local barrier) entry: save the state of the cell left,
-// load the entered cell and catch it up over the steps it was not observed
-// (UpdateBarrierStateEta, S.h:2025-2068 / D.h:2468-2517).  The catch-up
-// probability is evaluated in FP64 exactly as in the FP64 path.
-__device__ __noinline__ int f_enter_cell(const JobF* Jp, const SlotsDev S, int64_t slot, int64_t traj, bool dbl,
-                                         uint32_t g, int64_t key_prev, int state, int64_t key_cur, uint64_t s) {
-    const JobF& J = *Jp;
-    f_ring_store(J, S, slot, traj, key_prev, state, (int64_t)s);
-    int ps;
-    int64_t stamp;
-    f_ring_load(J, S, slot, dbl, g, key_cur, &ps, &stamp);
-    if (!J.eta) return ps;
-    const double lap = (double)((int64_t)s - stamp);
-    const double pl = J.c_lap[J.eq ? 0 : ps] * -expm1_f64(J.a_lap * lap);
-    const uint64_t Tl = prob_to_u64(pl);
-    const Words wc = philox_at(s, g, TAG_CATCHUP, J.key0, J.key1);
-    const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
-    return (U < Tl) ? (ps ^ 1) : ps;
-}
-
-__device__ __noinline__ bool f_refine_flip(const JobF* Jp, uint32_t g, uint64_t s, uint32_t tlo) {
-    const Words wr = philox_at(s, g, TAG_REFINE, Jp->key0, Jp->key1);
-    return wr.w0 < tlo;
-}
-
-// FP32 force constants of one job, kept in registers by the hot loop.
-struct ForceC {
-    float w, sl0, sl1;                       // single barrier
-    float xb0, xb1, lo0, hi1, xc;            // double barrier geometry
-    float n0[2], p0[2], n1[2], p1[2];        // double barrier slopes by state
-};
-
-__device__ __forceinline__ ForceC f_force_consts(const JobF& J) {
-    ForceC c;
-    c.w = J.w; c.sl0 = J.slope[0]; c.sl1 = J.slope[1];
-    c.xb0 = J.xb[0]; c.xb1 = J.xb[1]; c.lo0 = J.lo0; c.hi1 = J.hi1; c.xc = J.xc;
-    for (int s = 0; s < 2; ++s) { c.n0[s] = J.sN[0][s]; c.p0[s] = J.sP[0][s]; c.n1[s] = J.sN[1][s]; c.p1[s] = J.sP[1][s]; }
-    return c;
-}
-
-// FP32 force of the current state (EnergyAndForce, S.h:1292-1324 /
+// FP32 force of state st at xp (EnergyAndForce, S.h:1292-1324 /
 // D.h:1464-1522).
 template <bool DBL>
-__device__ __forceinline__ float f_force(const ForceC& c, float xp, int state) {
+__device__ __forceinline__ float force_of(const JobF& J, float xp, int st) {
     if (!DBL) {
         const float a = fabsf(xp);
-        const float sl = state ? c.sl1 : c.sl0;
-        return (a < c.w && a > 0.0f) ? copysignf(sl, xp) : 0.0f;
+        return (a < J.w && a > 0.0f) ? copysignf(J.slope[st], xp) : 0.0f;
     } else {
         float f = 0.0f;
-        if (xp < c.xb0 && xp > c.lo0) f = state ? c.n0[1] : c.n0[0];
-        if (xp < c.xc && xp > c.xb0) f = state ? c.p0[1] : c.p0[0];
-        if (xp < c.xb1 && xp > c.xc) f = state ? c.n1[1] : c.n1[0];
-        if (xp < c.hi1 && xp > c.xb1) f = state ? c.p1[1] : c.p1[0];
+        if (xp < J.xb[0] && xp > J.lo0) f = J.sN[0][st];
+        if (xp < J.xc && xp > J.xb[0]) f = J.sP[0][st];
+        if (xp < J.xb[1] && xp > J.xc) f = J.sN[1][st];
+        if (xp < J.hi1 && xp > J.xb[1]) f = J.sP[1][st];
         return -f;
     }
+}
+
+// Open band (lo, hi) of consecutive breakpoints around xp; lo = hi = xp when
+// xp sits on a breakpoint, so that the next step takes the general path.
+__device__ __forceinline__ void band_of(const JobF& J, float xp, float* lo, float* hi) {
+    float l = -__int_as_float(0x7f800000), h = __int_as_float(0x7f800000);
+    for (int i = 0; i < J.nbp; ++i) {
+        const float b = J.bp[i];
+        if (b < xp) { l = b; continue; }
+        if (b == xp) l = h = xp; else h = b;
+        break;
+    }
+    *lo = l;
+    *hi = h;
 }
 
 template <bool DBL>
@@ -150,158 +171,43 @@ __device__ void f_energy(const JobF& J, double xp, int s, double* E, double* B) 
     }
 }
 
+// WRITEX frame fields (velocity, force, barrier, energies, state).
 template <bool DBL>
-__device__ __noinline__ void f_record(const JobF* Jp, int64_t traj, int64_t frame, int cell, float xp, float v,
-                                      float F, int state) {
+__device__ __noinline__ void f_record_extra(const JobF* Jp, int64_t o, float xp, float v, float F, int state) {
     const JobF& J = *Jp;
+    double E, B;
+    f_energy<DBL>(J, (double)xp, state, &E, &B);
+    if (J.fv) J.fv[o] = (double)v;
+    if (J.ff) J.ff[o] = (double)F;
+    if (J.fb) J.fb[o] = B;
+    if (J.fpe) J.fpe[o] = E;
+    if (J.fke) J.fke[o] = J.mhalf * ((double)v * (double)v);
+    if (J.fst) J.fst[o] = (double)state;
+}
+
+template <bool DBL>
+__device__ __forceinline__ void f_record(const JobF& J, uint32_t traj, int64_t frame, int cell, float xp, float v,
+                                         float F, int state) {
     const int64_t o = frame * J.ntraj + traj;
-    const double x = (double)cell * J.Ld + (double)xp;
-    if (J.fx) J.fx[o] = x;
-    if (J.write_x) {
-        double E, B;
-        f_energy<DBL>(J, (double)xp, state, &E, &B);
-        if (J.fv) J.fv[o] = (double)v;
-        if (J.ff) J.ff[o] = (double)F;
-        if (J.fb) J.fb[o] = B;
-        if (J.fpe) J.fpe[o] = E;
-        if (J.fke) J.fke[o] = J.mhalf * ((double)v * (double)v);
-        if (J.fst) J.fst[o] = (double)state;
-    }
+    if (J.fx) J.fx[o] = (double)cell * J.Ld + (double)xp;
+    if (J.write_x) f_record_extra<DBL>(&J, o, xp, v, F, state);
 }
 
 __device__ __forceinline__ bool cg_hit32(int well, int size) { return (well % size) == 0; }
 
-// FPT initial-barrier bookkeeping (S.h:2187-2211, 2364-2388).
-__device__ void f_fpt_initial(const JobF& J, const SlotsDev& S, int64_t slot, uint32_t g, int64_t traj, int cell,
-                              int well, int state, uint32_t* bits) {
-    int s0, s1;
-    int64_t stamp;
-    if (well == cell) {
-        s0 = state;
-        J.init_idx0[traj] = cell;
-        f_ring_load(J, S, slot, false, g, (int64_t)cell + 1, &s1, &stamp);
-        J.init_idx1[traj] = cell + 1;
-    } else {
-        f_ring_load(J, S, slot, false, g, (int64_t)cell - 1, &s0, &stamp);
-        J.init_idx0[traj] = cell - 1;
-        s1 = state;
-        J.init_idx1[traj] = cell;
-    }
-    *bits = (*bits & ~(B_INIT0 | B_INIT1)) | (s0 ? B_INIT0 : 0u) | (s1 ? B_INIT1 : 0u);
-}
-
-__device__ __forceinline__ void f_fpt2_idx(const JobF& J, int64_t traj, int cell, int well) {
-    if (well == cell) { J.idx2_0[traj] = cell; J.idx2_1[traj] = cell + 1; }
-    else { J.idx2_0[traj] = cell - 1; J.idx2_1[traj] = cell; }
-}
-
-// Renewal statistics (UpdateStatistics, S.h:2334-2592 / D.h:2931-3209) with
-// integer step clocks.  Returns true when a FIRST_PASSAGE trajectory ends.
-template <bool DBL>
-__device__ __noinline__ bool f_events(const JobF* Jp, const SlotsDev S, int64_t slot, uint32_t g, int64_t traj,
-                                      uint64_t s, bool dWell, bool dCell, int cell, int well, int state) {
-    const JobF& J = *Jp;
-    const int64_t n = J.ntraj;
-    uint32_t bits = (uint32_t)J.bits[traj];
-    bool done = false;
-    const int64_t now = (int64_t)s;
-    if (!DBL && J.wt && !J.fp_mode) {
-        if (dWell) { J.wt_tick[traj] = now; bits |= B_WT_PASSED; }
-        else if (dCell && (bits & B_WT_PASSED)) {
-            int64_t& nwt = J.counts[(int64_t)LDP_C_WT * n + traj];
-            if (nwt < J.tick_cap) J.ticks[traj * J.tick_cap + nwt] = J.wt_tick[traj];
-            else J.counts[(int64_t)LDP_C_FLAGS * n + traj] |= LDP_FLAG_TICK_OVERFLOW;
-            nwt += 1;
-            bits &= ~B_WT_PASSED;
-        }
-    }
-    if (J.fpt || J.fp_mode) {
-        if (!DBL && !J.fp_mode) {
-            if ((bits & B_FPT_UP) && dCell) {
-                bits &= ~B_FPT_UP;
-                J.fpt_last[traj] = now;
-                f_fpt_initial(J, S, slot, g, traj, cell, well, state, &bits);
-            }
-            if (!(bits & B_FPT_UP) && dWell) {
-                bits |= B_FPT_UP;
-                if (J.counts[(int64_t)LDP_C_FPT * n + traj] == 0)
-                    J.ssum[(int64_t)LDP_S_FIRST_FPT * n + traj] = now - J.fpt_last[traj];
-                J.ssum[(int64_t)LDP_S_FPT * n + traj] += now - J.fpt_last[traj];
-                J.counts[(int64_t)LDP_C_FPT * n + traj] += 1;
-                const bool ib = (cell == J.init_idx0[traj]) ? ((bits & B_INIT0) != 0) : ((bits & B_INIT1) != 0);
-                J.counts[(int64_t)(ib ? LDP_C_INIT1 : LDP_C_INIT0) * n + traj] += 1;
-                J.counts[(int64_t)(state ? LDP_C_INST1 : LDP_C_INST0) * n + traj] += 1;
-            }
-        }
-        if ((bits & B_FPT2_UP) && dCell) {
-            bits &= ~B_FPT2_UP;
-            J.fpt2_last[traj] = now;
-            f_fpt2_idx(J, traj, cell, well);
-        }
-        if (dCell && !(bits & B_FPT2_UP) && J.idx2_0[traj] != cell && J.idx2_1[traj] != cell) {
-            if (J.counts[(int64_t)LDP_C_FPT2 * n + traj] == 0)
-                J.ssum[(int64_t)LDP_S_FIRST_FPT2 * n + traj] = now - J.fpt2_last[traj];
-            J.ssum[(int64_t)LDP_S_FPT2 * n + traj] += now - J.fpt2_last[traj];
-            J.counts[(int64_t)LDP_C_FPT2 * n + traj] += 1;
-            J.fpt2_last[traj] = now;
-            f_fpt2_idx(J, traj, cell, well);
-            if (J.fp_mode) done = true;
-        }
-    }
-    if (!DBL && J.tpt && !J.fp_mode) {
-        if (dCell) { bits &= ~B_TPT_UP; J.tpt_last[traj] = now; }
-        if (!(bits & B_TPT_UP) && dWell) {
-            bits |= B_TPT_UP;
-            if (J.counts[(int64_t)LDP_C_TPT * n + traj] == 0)
-                J.ssum[(int64_t)LDP_S_FIRST_TPT * n + traj] = now - J.tpt_last[traj];
-            J.ssum[(int64_t)LDP_S_TPT * n + traj] += now - J.tpt_last[traj];
-            J.counts[(int64_t)LDP_C_TPT * n + traj] += 1;
-        }
-        if (dCell) {
-            if (bits & B_TPT2_UP) bits &= ~B_TPT2_UP;
-            else if (well != J.tpt2_well[traj]) {
-                if (J.counts[(int64_t)LDP_C_TPT2 * n + traj] == 0)
-                    J.ssum[(int64_t)LDP_S_FIRST_TPT2 * n + traj] = now - J.tpt2_last[traj];
-                J.ssum[(int64_t)LDP_S_TPT2 * n + traj] += now - J.tpt2_last[traj];
-                J.counts[(int64_t)LDP_C_TPT2 * n + traj] += 1;
-            }
-            J.tpt2_last[traj] = now;
-            J.tpt2_well[traj] = well;
-        }
-    }
-    if (J.cg && !J.fp_mode && dCell) {
-        for (int jj = 0; jj < J.n_cg; ++jj) {
-            if (cg_hit32(well, J.cg_size[jj])) {
-                const int64_t o = (int64_t)jj * n + traj;
-                if (bits & (B_CG0 << jj)) {
-                    bits &= ~(B_CG0 << jj);
-                    J.cg_last[o] = now;
-                    J.cg_well[o] = well;
-                } else if (well != J.cg_well[o]) {
-                    J.ssum[(int64_t)(LDP_S_CG0 + jj) * n + traj] += now - J.cg_last[o];
-                    J.counts[(int64_t)(LDP_C_CG0 + jj) * n + traj] += 1;
-                    J.cg_last[o] = now;
-                    J.cg_well[o] = well;
-                }
-            }
-        }
-    }
-    J.bits[traj] = (int32_t)bits;
-    return done;
-}
-
 // Step 0 of a trajectory (IntegrateStep0 + InitializeBarrierState +
 // InitializeStatistics), FP64 where it is cheap and exact, then the hot
-// state is rounded to FP32.
+// state is rounded to FP32.  Writes the thread's rare state.
 template <bool DBL, bool OVER>
-__device__ __noinline__ void f_start(const JobF* Jp, const SlotsDev S, int64_t slot, int64_t traj, float* xp,
-                                     float* rv, int* cell, int* state, int* lb) {
+__device__ __noinline__ void f_start(const JobF* Jp, longlong2* ring, int64_t nslots, int ring_slots, int64_t slot,
+                                     uint32_t traj, RareSm* sm, int t, float* xp, float* rv, int* cell, int* state,
+                                     int* sw) {
     const JobF& J = *Jp;
-    const uint32_t g = (uint32_t)traj;
-    for (int r = 0; r < S.ring_slots; ++r) S.ring_tag[(int64_t)r * S.nslots + slot] = INT64_MIN;
+    const uint32_t g = traj;
+    for (int r = 0; r < ring_slots; ++r) ring[(int64_t)r * nslots + slot] = make_longlong2((long long)INT64_MIN, 0);
     const double red = J.x0 * J.invL;
-    const int64_t c = (int64_t)rint(red);
-    const int64_t well = (int64_t)floor(red);
+    const int c = (int)rint(red);
+    const int well = (int)floor(red);
     const double xpd = J.x0 - (double)c * J.Ld;
     int l = 0;
     if (DBL) l = (xpd < J.xcd) ? 0 : 1;
@@ -313,38 +219,50 @@ __device__ __noinline__ void f_start(const JobF* Jp, const SlotsDev S, int64_t s
     J.state0[traj] = st;
     J.v0s[traj] = v;
     uint32_t bits = 0;
+    int init0 = 0, idx2 = 0;
     if (J.at_bottom) {
-        if (!DBL && J.fpt && !J.fp_mode)
-            f_fpt_initial(J, S, slot, g, traj, (int)c, (int)well, st, &bits);
-        f_fpt2_idx(J, traj, (int)c, (int)well);
+        if (!DBL && J.fpt && !J.fp_mode) {
+            // FPT initial barrier pair (S.h:2187-2211); the ring is empty, so
+            // the neighbour has its default state.
+            int s0, s1;
+            if (well == c) { s0 = st; s1 = f_default_state(J, false, g, c + 1); init0 = c; }
+            else { s0 = f_default_state(J, false, g, c - 1); s1 = st; init0 = c - 1; }
+            bits |= (s0 ? B_INIT0 : 0u) | (s1 ? B_INIT1 : 0u);
+        }
+        idx2 = (well == c) ? c : c - 1;
     } else {
-        bits |= B_FPT_UP | B_FPT2_UP;
+        bits |= B_FPT_UP | B_FPT2_UP | B_TPT_UP | B_TPT2_UP;
     }
-    if (!J.at_bottom) bits |= B_TPT_UP | B_TPT2_UP;
-    J.tpt2_well[traj] = (int32_t)well;
-    J.fpt_last[traj] = 0;
-    J.fpt2_last[traj] = 0;
-    J.tpt_last[traj] = 0;
-    J.tpt2_last[traj] = 0;
-    J.wt_tick[traj] = 0;
     for (int j = 0; j < J.n_cg; ++j) {
         J.cg_last[(int64_t)j * J.ntraj + traj] = 0;
-        J.cg_well[(int64_t)j * J.ntraj + traj] = (int32_t)well;
-        if (!(J.at_bottom && cg_hit32((int)well, J.cg_size[j]))) bits |= (B_CG0 << j);
+        J.cg_well[(int64_t)j * J.ntraj + traj] = well;
+        if (!(J.at_bottom && cg_hit32(well, J.cg_size[j]))) bits |= (B_CG0 << j);
     }
-    J.bits[traj] = (int32_t)bits;
+    if (!DBL && J.wt) J.wt_tick[traj] = 0;
+    sm->bits[t] = bits;
+    sm->init0[t] = init0;
+    sm->idx2[t] = idx2;
+    sm->tpt2w[t] = well;
+    sm->ckey[t] = 0;
+    sm->cgw[t] = INT32_MIN;
+    sm->fidx[t] = 1;
+    sm->nxf[t] = (!J.fp_mode && J.freq_save) ? (long long)J.freq_save : INT64_MAX;
+    sm->fpt[t] = sm->fpt2[t] = sm->tpt[t] = sm->tpt2[t] = 0;
+    sm->cstamp[t] = 0;
+    sm->sc1[t] = 0;
+    sm->since[t] = 0;
     *xp = (float)xpd;
-    *cell = (int)c;
+    *cell = c;
     *state = st;
-    *lb = l;
+    *sw = l ? W_LB : 0;
     *rv = OVER ? (float)(J.sig_r_d * zr) : (float)v;
     if (!J.fp_mode) {
-        const float F = f_force<DBL>(f_force_consts(J), *xp, st);
-        f_record<DBL>(Jp, traj, 0, (int)c, *xp, OVER ? 0.0f : (float)v, F, st);
+        const float F = force_of<DBL>(J, *xp, st);
+        f_record<DBL>(J, traj, 0, c, *xp, OVER ? 0.0f : (float)v, F, st);
     }
 }
 
-__device__ __noinline__ void f_retire(const JobF* Jp, const SlotsDev S, int64_t traj, uint64_t steps_done,
+__device__ __noinline__ void f_retire(const JobF* Jp, unsigned long long* retired, uint32_t traj, uint64_t steps_done,
                                       int64_t sc1, int cell, float xp, float v, int state, uint32_t flags) {
     const JobF& J = *Jp;
     const int64_t n = J.ntraj;
@@ -356,195 +274,418 @@ __device__ __noinline__ void f_retire(const JobF* Jp, const SlotsDev S, int64_t 
     J.v_final[traj] = (double)v;
     J.state_final[traj] = state;
     atomicAdd(J.remaining, ~0ull);   // -1 modulo 2^64
-    atomicAdd(S.retired, 1ull);
+    atomicAdd(retired, 1ull);
 }
 
 // Resolves a claimed queue index to (job, trajectory).
-__device__ __noinline__ void f_resolve(const QueueDev q, int64_t idx, int* job, int64_t* traj) {
-    int lo = 0, hi = *(volatile int32_t*)q.nranges - 1;
+__device__ __noinline__ int64_t f_resolve(const int64_t* range_end, const int32_t* range_job,
+                                          const int64_t* range_first, const int32_t* nranges, int64_t idx, int* job) {
+    int lo = 0, hi = *(volatile const int32_t*)nranges - 1;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (q.range_end[mid] > idx) hi = mid; else lo = mid + 1;
+        if (range_end[mid] > idx) hi = mid; else lo = mid + 1;
     }
-    const int64_t begin = lo ? q.range_end[lo - 1] : 0;
-    *job = q.range_job[lo];
-    *traj = q.range_first[lo] + (idx - begin);
+    const int64_t begin = lo ? range_end[lo - 1] : 0;
+    *job = range_job[lo];
+    return range_first[lo] + (idx - begin);
+}
+
+// Steps from step s to the next frame (step nxf) or the last step.
+__device__ __forceinline__ int steps_to_special(const JobF& J, uint64_t s, long long nxf) {
+    const uint64_t e = (uint64_t)nxf < J.nsteps ? (uint64_t)nxf : J.nsteps;
+    const uint64_t d = e - s;
+    return (int)(d < (uint64_t)kLeftMax ? d : (uint64_t)kLeftMax);
+}
+
+// 1 - e^x for x <= 0 in FP32: a degree-5 Taylor polynomial of -expm1 on
+// (-1/32, 0] (truncation below 1e-10 relative), 1 - expf(x) below.
+__device__ __forceinline__ float one_minus_exp(float x) {
+    if (x > -0.03125f)
+        return -x * fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 120.0f, 1.0f / 24.0f), 1.0f / 6.0f), 0.5f), 1.0f);
+    return 1.0f - expf(x);
 }
 
 }  // namespace
 
 template <bool DBL, bool OVER>
-__global__ void __launch_bounds__(256) fp32_persistent_kernel(const QueueDev q, const SlotsDev S,
-                                                              uint64_t pair_budget) {
-    const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned lane = threadIdx.x & 31u;
-    const bool in_range = slot < S.nslots;
+__global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev q, const SlotsDev S,
+                                                                 uint32_t pair_budget) {
+    __shared__ RareSm sm;
+    const int t = threadIdx.x;
+    const int64_t slot = (int64_t)blockIdx.x * blockDim.x + t;
+    const unsigned lane = t & 31u;
+    const float kInf = __int_as_float(0x7f800000);
 
     // ---- slot state ----
-    int job = in_range ? S.job[slot] : -1;
-    int64_t traj = 0;
-    uint64_t s = 1;
-    float xp = 0.f, rv = 0.f;
-    int cell = 0, state = 0, lb = 0;
-    int64_t sc1 = 0;
+    int job = (slot < S.nslots) ? S.job[slot] : -1;
+    uint32_t traj = 0;
+    uint64_t j = 0;                 // next pair: steps 2j+1, 2j+2
+    float xp = 0.f, rv = 0.f, F = 0.f, lo = -kInf, hi = kInf;
+    uint32_t thi = 0;
+    int cell = 0, state = 0, sw = 0, left = kLeftMax;
+    float c1 = 0.f, c2 = 0.f, c3 = 0.f, kn = 0.f;
+    uint32_t key0 = 0, key1 = 0;
+
+    // Per-job constants into registers; band, force and countdown from the
+    // position.  s = next step.
+    auto bind = [&](uint64_t s) {
+        const JobF& J = q.jobs[job];
+        if (OVER) c1 = J.c_drift;
+        else { c1 = J.hdt_invM; c2 = J.hdt; c3 = J.expg; }
+        kn = J.bm_k;
+        key0 = J.key0;
+        key1 = J.key1;
+        thi = thi_of(J, state);
+        band_of(J, xp, &lo, &hi);
+        F = force_of<DBL>(J, xp, state);
+        left = steps_to_special(J, s - 1, sm.nxf[t]);
+        j = (s - 1) >> 1;
+    };
+
     if (job >= 0) {
-        traj = S.traj[slot];
-        s = (uint64_t)S.step[slot];
+        const JobF& J = q.jobs[job];
+        traj = (uint32_t)S.traj[slot];
+        const uint64_t s = (uint64_t)S.step[slot];
         xp = S.xp[slot];
         rv = S.rv[slot];
         cell = S.cell[slot];
         const int st = S.st[slot];
         state = st & 1;
-        lb = (st >> 1) & 1;
-        sc1 = S.sc1[slot];
+        sw = st >> 1;
+        sm.bits[t] = (uint32_t)J.bits[traj];
+        sm.init0[t] = J.init_idx0[traj];
+        sm.idx2[t] = J.idx2_0[traj];
+        sm.tpt2w[t] = J.tpt2_well[traj];
+        sm.fpt[t] = J.fpt_last[traj];
+        sm.fpt2[t] = J.fpt2_last[traj];
+        sm.tpt[t] = J.tpt_last[traj];
+        sm.tpt2[t] = J.tpt2_last[traj];
+        sm.ckey[t] = S.ckey[slot];
+        sm.cstamp[t] = S.cstamp[slot];
+        sm.sc1[t] = S.sc1[slot];
+        sm.since[t] = S.since[slot];
+        sm.cgw[t] = S.cgw[slot];
+        sm.fidx[t] = S.fidx[slot];
+        sm.nxf[t] = S.nxf[slot];
+        bind(s);
     }
-    // Hot per-job constants in registers.
-    const JobF* J = nullptr;
-    float L = 0.f, halfL = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f;
-    ForceC fc{};
-    uint32_t key0 = 0, key1 = 0, thi0 = 0, thi1 = 0, g = 0;
-    uint64_t nsteps = 0, fs = 0, to_rec = 0;
-    int well = 0;
-    float F = 0.f;
-    auto bind = [&]() {
-        J = &q.jobs[job];
-        L = J->L; halfL = J->halfL;
-        if (OVER) { c1 = J->c_drift; c2 = J->sig_r; }
-        else { c1 = J->hdt_invM; c2 = J->hdt; c3 = J->expg; c4 = J->sig_v; }
-        fc = f_force_consts(*J);
-        key0 = J->key0; key1 = J->key1;
-        const uint64_t T0 = J->eq ? J->T_eq : J->T_as[0];
-        const uint64_t T1 = J->eq ? J->T_eq : J->T_as[1];
-        thi0 = (uint32_t)(T0 >> 32);
-        thi1 = (uint32_t)(T1 >> 32);
-        nsteps = J->nsteps;
-        fs = J->fp_mode ? 0 : J->freq_save;
-        g = (uint32_t)traj;
-        well = cell - (xp < 0.0f ? 1 : 0);
-        F = f_force<DBL>(fc, xp, state);
-        to_rec = fs ? fs - ((s - 1) % fs) : ~0ull;
+
+    // End of a trajectory after step `done` (v: velocity after that step).
+    auto retire = [&](const JobF& J, uint64_t done, float v, uint32_t flags) {
+        const int64_t sc1 = sm.sc1[t] + (state ? (int64_t)done + 1 - sm.since[t] : 0);
+        if (J.fp_mode && !(flags & LDP_FLAG_NONFINITE) && !(sm.bits[t] & B_HAS_FPT2)) flags |= LDP_FLAG_CENSORED;
+        f_retire(&J, S.retired, traj, done, sc1, cell, xp, OVER ? 0.0f : v, state, flags);
+        job = -1;
+        lo = -kInf;
+        hi = kInf;
+        thi = 0;
+        F = 0.f;
+        left = kLeftMax;
     };
-    if (job >= 0) bind();
+
+    // Cell (double model: local barrier) entry: write the state of the key
+    // left through to the ring, take the entered key's state and stamp from
+    // the one-entry cache or the ring, and catch it up over the steps it was
+    // not observed (UpdateBarrierStateEta, S.h:2025-2068 / D.h:2468-2517;
+    // probability in FP64 as in the FP64 path).
+    auto enter = [&](const JobF& J, uint64_t s, int key_prev, int st, int key_cur) -> int {
+        const int64_t n = J.ntraj;
+        const int rmask = S.ring_slots - 1;
+        if (sw & W_EVICT) red_add(&J.counts[(int64_t)LDP_C_EVICT * n + traj], 1);
+        S.ring[(int64_t)(key_prev & rmask) * S.nslots + slot] =
+            make_longlong2((long long)key_prev, (long long)((s << 1) | (uint64_t)st));
+        int ps;
+        int64_t stamp;
+        bool ev = false;
+        if ((sw & W_CVALID) && sm.ckey[t] == key_cur) {
+            ps = (sw & W_CSTATE) ? 1 : 0;
+            stamp = sm.cstamp[t];
+        } else {
+            const longlong2 e = S.ring[(int64_t)(key_cur & rmask) * S.nslots + slot];
+            if (e.x == (long long)key_cur) {
+                ps = (int)(e.y & 1);
+                stamp = e.y >> 1;
+            } else {
+                ps = f_default_state(J, DBL, traj, key_cur);
+                stamp = 0;
+                ev = e.x != (long long)INT64_MIN;
+            }
+        }
+        sm.ckey[t] = key_prev;
+        sm.cstamp[t] = (long long)s;
+        sw = (sw & W_LB) | W_CVALID | (st ? W_CSTATE : 0) | (ev ? W_EVICT : 0);
+        if (!J.eta) return ps;
+        // Flip with probability c (1 - e^{a lap}), FP32, against the high
+        // word of the same catch-up uniform the FP64 path draws.
+        const float pl = J.c_lapf[J.eq ? 0 : ps] * one_minus_exp(J.a_lapf * (float)((int64_t)s - stamp));
+        const uint32_t w0 = philox_at(s, traj, TAG_CATCHUP, J.key0, J.key1).w0;
+        const bool flip = (pl >= 1.0f) || (w0 < (uint32_t)(pl * 4294967296.0f));
+        return flip ? (ps ^ 1) : ps;
+    };
+
+    // Renewal statistics (UpdateStatistics, S.h:2334-2592 / D.h:2931-3209)
+    // with integer step clocks.  Returns true when a FIRST_PASSAGE
+    // trajectory ends.
+    auto events = [&](const JobF& J, int64_t now, bool dWell, bool dCell, int well) -> bool {
+        const int64_t n = J.ntraj;
+        int64_t* C = J.counts;
+        int64_t* U = J.ssum;
+        uint32_t bits = sm.bits[t];
+        bool done = false;
+        if (!DBL && J.wt && !J.fp_mode) {
+            if (dWell) { J.wt_tick[traj] = now; bits |= B_WT_PASSED; }
+            else if (dCell && (bits & B_WT_PASSED)) {
+                int64_t& nwt = C[(int64_t)LDP_C_WT * n + traj];
+                if (nwt < J.tick_cap) J.ticks[(int64_t)traj * J.tick_cap + nwt] = J.wt_tick[traj];
+                else C[(int64_t)LDP_C_FLAGS * n + traj] |= LDP_FLAG_TICK_OVERFLOW;
+                nwt += 1;
+                bits &= ~B_WT_PASSED;
+            }
+        }
+        if (J.fpt || J.fp_mode) {
+            if (!DBL && !J.fp_mode) {
+                if ((bits & B_FPT_UP) && dCell) {
+                    // initial barrier pair (S.h:2364-2388)
+                    bits &= ~(B_FPT_UP | B_INIT0 | B_INIT1);
+                    sm.fpt[t] = now;
+                    int s0, s1, i0;
+                    if (well == cell) { s0 = state; s1 = f_ring_state(J, S, slot, false, traj, cell + 1); i0 = cell; }
+                    else { s0 = f_ring_state(J, S, slot, false, traj, cell - 1); s1 = state; i0 = cell - 1; }
+                    sm.init0[t] = i0;
+                    bits |= (s0 ? B_INIT0 : 0u) | (s1 ? B_INIT1 : 0u);
+                }
+                if (!(bits & B_FPT_UP) && dWell) {
+                    bits |= B_FPT_UP;
+                    const int64_t d = now - sm.fpt[t];
+                    if (!(bits & B_HAS_FPT)) { bits |= B_HAS_FPT; U[(int64_t)LDP_S_FIRST_FPT * n + traj] = d; }
+                    red_add(&U[(int64_t)LDP_S_FPT * n + traj], d);
+                    red_add(&C[(int64_t)LDP_C_FPT * n + traj], 1);
+                    const bool ib = (cell == sm.init0[t]) ? ((bits & B_INIT0) != 0) : ((bits & B_INIT1) != 0);
+                    red_add(&C[(int64_t)(ib ? LDP_C_INIT1 : LDP_C_INIT0) * n + traj], 1);
+                    red_add(&C[(int64_t)(state ? LDP_C_INST1 : LDP_C_INST0) * n + traj], 1);
+                }
+            }
+            if ((bits & B_FPT2_UP) && dCell) {
+                bits &= ~B_FPT2_UP;
+                sm.fpt2[t] = now;
+                sm.idx2[t] = (well == cell) ? cell : cell - 1;
+            }
+            const int i2 = sm.idx2[t];
+            if (dCell && !(bits & B_FPT2_UP) && i2 != cell && i2 + 1 != cell) {
+                const int64_t d = now - sm.fpt2[t];
+                if (!(bits & B_HAS_FPT2)) { bits |= B_HAS_FPT2; U[(int64_t)LDP_S_FIRST_FPT2 * n + traj] = d; }
+                red_add(&U[(int64_t)LDP_S_FPT2 * n + traj], d);
+                red_add(&C[(int64_t)LDP_C_FPT2 * n + traj], 1);
+                sm.fpt2[t] = now;
+                sm.idx2[t] = (well == cell) ? cell : cell - 1;
+                if (J.fp_mode) done = true;
+            }
+        }
+        if (!DBL && J.tpt && !J.fp_mode) {
+            if (dCell) { bits &= ~B_TPT_UP; sm.tpt[t] = now; }
+            if (!(bits & B_TPT_UP) && dWell) {
+                bits |= B_TPT_UP;
+                const int64_t d = now - sm.tpt[t];
+                if (!(bits & B_HAS_TPT)) { bits |= B_HAS_TPT; U[(int64_t)LDP_S_FIRST_TPT * n + traj] = d; }
+                red_add(&U[(int64_t)LDP_S_TPT * n + traj], d);
+                red_add(&C[(int64_t)LDP_C_TPT * n + traj], 1);
+            }
+            if (dCell) {
+                if (bits & B_TPT2_UP) bits &= ~B_TPT2_UP;
+                else if (well != sm.tpt2w[t]) {
+                    const int64_t d = now - sm.tpt2[t];
+                    if (!(bits & B_HAS_TPT2)) { bits |= B_HAS_TPT2; U[(int64_t)LDP_S_FIRST_TPT2 * n + traj] = d; }
+                    red_add(&U[(int64_t)LDP_S_TPT2 * n + traj], d);
+                    red_add(&C[(int64_t)LDP_C_TPT2 * n + traj], 1);
+                }
+                sm.tpt2[t] = now;
+                sm.tpt2w[t] = well;
+            }
+        }
+        // An FPTCG evaluation at the well of the previous one changes nothing
+        // (every entry it hits already holds that well), so it is skipped.
+        if (J.cg && !J.fp_mode && dCell && well != sm.cgw[t]) {
+            sm.cgw[t] = well;
+            for (int jj = 0; jj < J.n_cg; ++jj) {
+                if (cg_hit32(well, J.cg_size[jj])) {
+                    const int64_t o = (int64_t)jj * n + traj;
+                    if (bits & (B_CG0 << jj)) {
+                        bits &= ~(B_CG0 << jj);
+                        J.cg_last[o] = now;
+                        J.cg_well[o] = well;
+                    } else if (well != J.cg_well[o]) {
+                        red_add(&U[(int64_t)(LDP_S_CG0 + jj) * n + traj], now - J.cg_last[o]);
+                        red_add(&C[(int64_t)(LDP_C_CG0 + jj) * n + traj], 1);
+                        J.cg_last[o] = now;
+                        J.cg_well[o] = well;
+                    }
+                }
+            }
+        }
+        sm.bits[t] = bits;
+        return done;
+    };
+
+    // The general step s (position already advanced with flip word fw):
+    // the FP64 step order of ldp_fp64.cu from the index update on.
+    auto general = [&](uint64_t s, uint32_t fw) {
+        if (job < 0) return;
+        const JobF& J = q.jobs[job];
+        if (!(fabsf(xp) < kInf)) {
+            retire(J, s - 1, rv, LDP_FLAG_NONFINITE);
+            return;
+        }
+        const int cell_prev = cell;
+        const int lb_prev = sw & W_LB;
+        const int well_prev = cell_prev - (lo < 0.0f ? 1 : 0);
+        const bool moved = !(xp > lo && xp < hi);
+        if (moved) {
+            if (xp >= J.halfL) { xp -= J.L; ++cell; }
+            else if (xp < -J.halfL) { xp += J.L; --cell; }
+            if (!(xp >= -J.halfL && xp < J.halfL)) {
+                // more than one cell in one step
+                const float k = floorf(xp * J.invLf + 0.5f);
+                xp = fmaf(-k, J.L, xp);
+                cell += (int)k;
+                if (xp >= J.halfL) { xp -= J.L; ++cell; }
+                else if (xp < -J.halfL) { xp += J.L; --cell; }
+            }
+        }
+        const int well = cell - (xp < 0.0f ? 1 : 0);
+        const int lb = DBL ? (xp < J.xc ? 0 : 1) : 0;
+        const bool dCell = cell != cell_prev;
+        const bool dWell = well != well_prev;
+        const bool dKey = DBL ? (lb != lb_prev) : dCell;
+        int st = state;
+        if (fw <= thi) {
+            bool flip = fw < thi;
+            if (fw == thi) {
+                const uint64_t T = J.eq ? J.T_eq : J.T_as[st];
+                flip = philox_at(s, traj, TAG_REFINE, J.key0, J.key1).w0 < (uint32_t)T;
+            }
+            st ^= (int)flip;
+        }
+        if (dKey) st = enter(J, s, fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb));
+        if (DBL) sw = (sw & ~W_LB) | (lb ? W_LB : 0);
+        if (st != state) {
+            if (st) sm.since[t] = (long long)s;
+            else sm.sc1[t] += (long long)s - sm.since[t];
+            state = st;
+            thi = thi_of(J, st);
+        }
+        band_of(J, xp, &lo, &hi);
+        F = force_of<DBL>(J, xp, state);
+        bool finish = false;
+        if (dCell || dWell) finish = events(J, (int64_t)s, dWell, dCell, well);
+        const float vk = OVER ? 0.0f : fmaf(F, c1, rv);
+        if (left == 0) {
+            if ((long long)s == sm.nxf[t]) {
+                f_record<DBL>(J, traj, sm.fidx[t], cell, xp, vk, F, state);
+                sm.fidx[t] += 1;
+                sm.nxf[t] += (long long)J.freq_save;
+            }
+            if (s == J.nsteps) finish = true;
+            left = steps_to_special(J, s, sm.nxf[t]);
+        }
+        if (finish) retire(J, s, vk, 0);
+    };
 
     bool dry = false;   // the queue had nothing left for this warp
-    uint32_t flags = 0;
-    for (uint64_t it = 0; it < pair_budget; ++it) {
-        // ---- warp-aggregated refill ----
-        const bool need = in_range && job < 0 && !dry;
-        const unsigned m = __ballot_sync(kFull, need);
-        if (m) {
-            const int leader = __ffs(m) - 1;
-            unsigned long long base = 0, got = 0;
-            if ((int)lane == leader) {
-                const unsigned long long tail = *(volatile unsigned long long*)q.tail;
-                unsigned long long old = *(volatile unsigned long long*)q.head;
-                for (int tries = 0; tries < kClaimTries; ++tries) {
-                    if (old >= tail) break;
-                    const unsigned long long want = min((unsigned long long)__popc(m), tail - old);
-                    const unsigned long long prev = atomicCAS(q.head, old, old + want);
-                    if (prev == old) { base = old; got = want; break; }
-                    old = prev;
+    for (uint32_t it = 0; it < pair_budget; ++it) {
+        // ---- warp-aggregated refill of idle lanes ----
+        const unsigned idle = __ballot_sync(kFull, job < 0);
+        if (idle) {
+            const bool need = job < 0 && !dry && slot < S.nslots;
+            const unsigned m = __ballot_sync(kFull, need);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned long long base = 0, got = 0;
+                if ((int)lane == leader) {
+                    const unsigned long long tail = *(volatile unsigned long long*)q.tail;
+                    unsigned long long old = *(volatile unsigned long long*)q.head;
+                    for (int tries = 0; tries < kClaimTries; ++tries) {
+                        if (old >= tail) break;
+                        const unsigned long long want = min((unsigned long long)__popc(m), tail - old);
+                        const unsigned long long prev = atomicCAS(q.head, old, old + want);
+                        if (prev == old) { base = old; got = want; break; }
+                        old = prev;
+                    }
+                }
+                base = __shfl_sync(kFull, base, leader);
+                got = __shfl_sync(kFull, got, leader);
+                if (got < (unsigned long long)__popc(m)) dry = true;
+                if (need) {
+                    const unsigned rank = __popc(m & ((1u << lane) - 1u));
+                    if (rank < got) {
+                        traj = (uint32_t)f_resolve(q.range_end, q.range_job, q.range_first, q.nranges,
+                                                   (int64_t)(base + rank), &job);
+                        const JobF* Jn = &q.jobs[job];
+                        f_start<DBL, OVER>(Jn, S.ring, S.nslots, S.ring_slots, slot, traj, &sm, t, &xp, &rv, &cell,
+                                           &state, &sw);
+                        bind(1);
+                        if (Jn->nsteps == 0) retire(*Jn, 0, rv, 0);
+                    }
                 }
             }
-            base = __shfl_sync(kFull, base, leader);
-            got = __shfl_sync(kFull, got, leader);
-            if (got < (unsigned long long)__popc(m)) dry = true;
-            if (need) {
-                const unsigned rank = __popc(m & ((1u << lane) - 1u));
-                if (rank < got) {
-                    int64_t t;
-                    f_resolve(q, (int64_t)(base + rank), &job, &t);
-                    traj = t;
-                    f_start<DBL, OVER>(&q.jobs[job], S, slot, traj, &xp, &rv, &cell, &state, &lb);
-                    s = 1;
-                    sc1 = state;
-                    flags = 0;
-                    bind();
-                }
+            if (__all_sync(kFull, job < 0)) {
+                if (dry || m == 0) break;
+                continue;
             }
+            if (job < 0) continue;
         }
-        if (__all_sync(kFull, job < 0)) {
-            if (dry || !__any_sync(kFull, need)) break;
-            continue;
-        }
-        if (job < 0) continue;
 
-        // ---- one Philox call, two steps ----
-        const uint64_t j = (s - 1) >> 1;
-        const Words w = philox((uint32_t)j, (uint32_t)(j >> 32), g, TAG_STEP, key0, key1);
-        float za, zb;
-        gauss_pair_f32(w.w0, w.w1, &za, &zb);
-        bool finished = false;
+        // ---- one Philox block, two steps ----
+        const Words w = philox((uint32_t)j, (uint32_t)(j >> 32), traj, TAG_STEP, key0, key1);
+        float n0, n1;
+        noise_pair(w.w0, w.w1, kn, &n0, &n1);
+        const uint64_t s0 = 2 * j + 1;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            if (h == 1 && (finished || s > nsteps)) break;
-            const float z = h ? zb : za;
+            const float nz = h ? n1 : n0;
             const uint32_t fw = h ? w.w3 : w.w2;
-            const int cell_prev = cell, well_prev = well, lb_prev = lb;
             if (OVER) {
-                const float rf = c2 * z;
                 xp = fmaf(F, c1, xp);
-                xp = xp + rf;
+                xp = xp + nz;
                 xp = xp + rv;
-                rv = rf;
+                rv = nz;
             } else {
                 rv = fmaf(F, c1, rv);
                 xp = fmaf(rv, c2, xp);
-                rv = fmaf(c3, rv, c4 * z);
+                rv = fmaf(c3, rv, nz);
                 xp = fmaf(rv, c2, xp);
             }
-            if (!isfinite(xp)) {
-                flags |= LDP_FLAG_NONFINITE;
-                finished = true;
-                break;
-            }
-            if (xp >= halfL) { xp -= L; ++cell; }
-            else if (xp < -halfL) { xp += L; --cell; }
-            well = cell - (xp < 0.0f ? 1 : 0);
-            if (DBL) lb = (xp < fc.xc) ? 0 : 1;
-            const bool dCell = cell != cell_prev;
-            const bool dWell = well != well_prev;
-            const bool dKey = DBL ? (lb != lb_prev) : dCell;
-            // per-step dichotomic flip: 64-bit Bernoulli, high word first
-            const uint32_t thi = state ? thi1 : thi0;
-            bool flip = fw < thi;
-            if (fw == thi) {
-                const uint64_t T = J->eq ? J->T_eq : J->T_as[state];
-                flip = f_refine_flip(J, g, s, (uint32_t)T);
-            }
-            state ^= (int)flip;
-            if (dKey)
-                state = f_enter_cell(J, S, slot, traj, DBL, g, fkey(DBL, cell_prev, lb_prev), state,
-                                     fkey(DBL, cell, lb), s);
-            sc1 += state;
-            F = f_force<DBL>(fc, xp, state);
+            --left;
+            if (!(xp > lo && xp < hi) || fw <= thi || left == 0) general(s0 + h, fw);
             if (!OVER) rv = fmaf(F, c1, rv);
-            if (dCell || dWell) finished = f_events<DBL>(J, S, slot, g, traj, s, dWell, dCell, cell, well, state);
-            if (--to_rec == 0) {
-                f_record<DBL>(J, traj, (int64_t)(s / fs), cell, xp, OVER ? 0.0f : rv, F, state);
-                to_rec = fs;
-            }
-            if (s == nsteps) finished = true;
-            ++s;
         }
-        if (finished) {
-            const uint64_t done = s - 1;
-            if (J->fp_mode && !(flags & LDP_FLAG_NONFINITE) && J->counts[(int64_t)LDP_C_FPT2 * J->ntraj + traj] == 0)
-                flags |= LDP_FLAG_CENSORED;
-            f_retire(J, S, traj, done, sc1, cell, xp, OVER ? (float)0.0f : rv, state, flags);
-            job = -1;
-        }
+        ++j;
     }
-    if (!in_range) return;
+
+    if (slot >= S.nslots) return;
     S.job[slot] = job;
     if (job >= 0) {
+        const JobF& J = q.jobs[job];
         S.traj[slot] = traj;
-        S.step[slot] = (int64_t)s;
+        S.step[slot] = (int64_t)(2 * j + 1);
         S.xp[slot] = xp;
         S.rv[slot] = rv;
         S.cell[slot] = cell;
-        S.st[slot] = state | (lb << 1);
-        S.sc1[slot] = sc1;
+        S.st[slot] = state | (sw << 1);
+        S.ckey[slot] = sm.ckey[t];
+        S.cstamp[slot] = sm.cstamp[t];
+        S.sc1[slot] = sm.sc1[t];
+        S.since[slot] = sm.since[t];
+        S.cgw[slot] = sm.cgw[t];
+        S.fidx[slot] = sm.fidx[t];
+        S.nxf[slot] = sm.nxf[t];
+        J.bits[traj] = (int32_t)sm.bits[t];
+        J.init_idx0[traj] = sm.init0[t];
+        J.idx2_0[traj] = sm.idx2[t];
+        J.tpt2_well[traj] = sm.tpt2w[t];
+        J.fpt_last[traj] = sm.fpt[t];
+        J.fpt2_last[traj] = sm.fpt2[t];
+        J.tpt_last[traj] = sm.tpt[t];
+        J.tpt2_last[traj] = sm.tpt2[t];
     }
 }
 
@@ -558,9 +699,10 @@ int fp32_blocks_per_sm(bool dbl, bool over, int block) {
     return e == cudaSuccess ? n : 0;
 }
 
-int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint64_t pair_budget, int grid,
+int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint32_t pair_budget, int grid,
                            int block, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
+    if (block > kMaxBlock) return (int)cudaErrorInvalidValue;
     if (dbl) {
         if (over) fp32_persistent_kernel<true, true><<<grid, block, 0, st>>>(q, s, pair_budget);
         else fp32_persistent_kernel<true, false><<<grid, block, 0, st>>>(q, s, pair_budget);

@@ -11,6 +11,7 @@
 // (seed, job id, trajectory, step).
 #pragma once
 #include <cstdint>
+#include <vector_types.h>
 #include "ldp_engine.h"
 
 namespace ldp {
@@ -28,6 +29,11 @@ struct JobF {
     // FP32 step constants
     float L, halfL, w, slope[2], xb[2], lo0, hi1, xc, sN[2][2], sP[2][2];
     float c_drift, sig_r, hdt_invM, hdt, expg, sig_v;
+    float bm_k;          // Box-Muller radius scale: -2 ln2 sigma^2 (sigma of the step noise)
+    float a_lapf, c_lapf[2];  // catch-up flip probability c (1 - e^{a lap}) in FP32
+    float invLf;         // 1 / L
+    float bp[8];         // force breakpoints in [-L/2, L/2], ascending (cell edges included)
+    int32_t nbp, pad1;
     // FP64 constants (step 0, events, frames)
     double x0, v0, dt, Ld, invL, sig_v0, sig_r_d, a_lap, c_lap[2], p_first, p_cell0, mhalf;
     double Hs[2], Hd[2][2], iN[2][2], iP[2][2], sNd[2][2], sPd[2][2], wd, xbd[2], lo0d, hi1d, xcd;
@@ -68,19 +74,22 @@ struct SlotsDev {
     int64_t nslots;
     int32_t* job;           // -1: no trajectory
     int64_t* traj;
-    int64_t* step;          // next step to integrate
+    int64_t* step;          // next step to integrate (odd: launches end on step pairs)
     float *xp, *rv;         // rv: R_prev (overdamped) or v (underdamped)
-    int32_t *cell, *st;     // st: state | lb << 1
-    int64_t *sc0, *sc1;
-    int64_t* ring_tag;      // [R][nslots]
-    int64_t* ring_data;
+    int32_t *cell, *st;     // st: state | slot flags << 1 (local barrier, cache, eviction)
+    int32_t* ckey;          // key of the cell left last (cached state)
+    int64_t* cstamp;        // step at which it was left
+    int64_t *sc1, *since;   // completed state-1 steps; start of the current state-1 run
+    int32_t *cgw, *fidx;    // well of the last FPTCG evaluation; index of the next frame
+    int64_t* nxf;           // step of the next frame
+    longlong2* ring;        // [R][nslots] cell table: {key, stamp << 1 | state}
     unsigned long long* retired;   // total retired trajectories (all jobs)
     int32_t ring_slots;
 };
 
 // Resident blocks per SM of the persistent kernel (0 on error).
 int fp32_blocks_per_sm(bool dbl, bool over, int block);
-int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint64_t pair_budget,
+int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint32_t pair_budget,
                            int grid, int block, void* stream);
 
 }  // namespace ldp

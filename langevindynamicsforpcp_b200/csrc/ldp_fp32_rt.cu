@@ -71,8 +71,8 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     Q.q.jobs = (JobF*)(a + o);
     // slots
     const int R = ring_slots;
-    size_t sb = al256(sizeof(int32_t) * nslots) * 3 + al256(sizeof(int64_t) * nslots) * 4 +
-                al256(sizeof(float) * nslots) * 2 + al256(sizeof(int64_t) * (size_t)R * nslots) * 2 +
+    size_t sb = al256(sizeof(int32_t) * nslots) * 6 + al256(sizeof(int64_t) * nslots) * 6 +
+                al256(sizeof(float) * nslots) * 2 + al256(sizeof(longlong2) * (size_t)R * nslots) +
                 al256(sizeof(unsigned long long));
     e = cudaMalloc(&Q.smem, sb);
     if (e != cudaSuccess) return (int)e;
@@ -85,14 +85,18 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     S.job = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
     S.cell = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
     S.st = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.ckey = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.cgw = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.fidx = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.nxf = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.traj = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.step = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.sc0 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.cstamp = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.sc1 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.since = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.xp = (float*)(a + o); o += al256(sizeof(float) * nslots);
     S.rv = (float*)(a + o); o += al256(sizeof(float) * nslots);
-    S.ring_tag = (int64_t*)(a + o); o += al256(sizeof(int64_t) * (size_t)R * nslots);
-    S.ring_data = (int64_t*)(a + o); o += al256(sizeof(int64_t) * (size_t)R * nslots);
+    S.ring = (longlong2*)(a + o); o += al256(sizeof(longlong2) * (size_t)R * nslots);
     S.retired = (unsigned long long*)(a + o);
     // every slot starts empty
     std::vector<int32_t> neg((size_t)nslots, -1);
@@ -127,6 +131,29 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
         }
     J->c_drift = k.fc_drift; J->sig_r = k.fsig_r; J->hdt_invM = k.fhdt_invM; J->hdt = k.fhdt;
     J->expg = k.fexpg; J->sig_v = k.fsig_v;
+    {
+        const double sg = k.over ? (double)k.fsig_r : (double)k.fsig_v;
+        J->bm_k = (float)(-2.0 * 0.69314718055994530942 * sg * sg);
+        J->invLf = (float)(1.0 / (double)k.fL);
+        J->a_lapf = (float)k.a_lap;
+        J->c_lapf[0] = (float)k.c_lap[0];
+        J->c_lapf[1] = (float)k.c_lap[1];
+        // Breakpoints of the FP32 force (the comparisons of the kernel's
+        // force_of use exactly these floats), the barrier top 0 (well
+        // boundary) and the cell edges.
+        float c[8];
+        int nc = 0;
+        c[nc++] = -k.fhalfL;
+        c[nc++] = k.fhalfL;
+        c[nc++] = 0.0f;
+        if (!k.dbl) { c[nc++] = -k.fw; c[nc++] = k.fw; }
+        else { c[nc++] = k.flo0; c[nc++] = k.fxb[0]; c[nc++] = k.fxc; c[nc++] = k.fxb[1]; c[nc++] = k.fhi1; }
+        std::sort(c, c + nc);
+        int nb = 0;
+        for (int i = 0; i < nc; ++i)
+            if (c[i] >= -k.fhalfL && c[i] <= k.fhalfL && (nb == 0 || c[i] != J->bp[nb - 1])) J->bp[nb++] = c[i];
+        J->nbp = nb;
+    }
     J->x0 = k.x0; J->v0 = k.v0; J->dt = k.dt; J->Ld = k.L; J->invL = k.invL; J->sig_v0 = k.sig_v0;
     J->sig_r_d = k.sig_r; J->a_lap = k.a_lap; J->c_lap[0] = k.c_lap[0]; J->c_lap[1] = k.c_lap[1];
     J->p_first = k.p_first; J->p_cell0 = k.p_cell0; J->mhalf = k.mhalf;
@@ -216,7 +243,8 @@ int fp32_pump(ldp_job* job, int nlaunch) {
     Fp32Queue& Q = ctx->fp32->q[job->fp32_type];
     const bool dbl = job->k.dbl, over = job->k.over;
     for (int i = 0; i < nlaunch; ++i) {
-        int e = launch_fp32_persistent(dbl, over, Q.q, Q.s, Q.pair_budget, Q.grid, Q.block, ctx->stream);
+        const uint32_t pb = (uint32_t)std::min<uint64_t>(Q.pair_budget, 0xffffffffull);
+        int e = launch_fp32_persistent(dbl, over, Q.q, Q.s, pb, Q.grid, Q.block, ctx->stream);
         if (e) return e;
         ++job->launches;
     }
