@@ -44,6 +44,22 @@ __device__ __forceinline__ Words philox(uint32_t c0, uint32_t c1, uint32_t c2, u
     return Words{c0, c1, c2, c3};
 }
 
+// The same function written with 32 x 32 -> 64-bit products (one wide
+// multiply per product gives both halves); identical output.
+__device__ __forceinline__ Words philox_wide(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                             uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint64_t p0 = (uint64_t)c0 * 0xD2511F53u;
+        const uint64_t p1 = (uint64_t)c2 * 0xCD9E8D57u;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0; c1 = (uint32_t)p1; c2 = n2; c3 = (uint32_t)p0;
+    }
+    return Words{c0, c1, c2, c3};
+}
+
 __device__ __forceinline__ Words philox_at(uint64_t a, uint32_t g, uint32_t tag, uint32_t k0, uint32_t k1) {
     return philox((uint32_t)a, (uint32_t)(a >> 32), g, tag, k0, k1);
 }

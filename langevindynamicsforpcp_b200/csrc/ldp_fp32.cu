@@ -33,7 +33,7 @@
 // Batching: each thread is a slot that owns one trajectory; when it retires
 // (fixed step count reached, or first passage in FIRST_PASSAGE mode) the
 // warp's idle lanes claim new trajectories from the device work queue with
-// one compare-and-swap per warp and a ballot/popc prefix.
+// one fetch-and-add per warp and a ballot/popc prefix.
 #include <cuda_runtime.h>
 
 #include "ldp_device.cuh"
@@ -44,7 +44,6 @@ namespace ldp {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kClaimTries = 1 << 16;   // bound of the claim retry loop
 constexpr int kMaxBlock = 256;
 constexpr int kLeftMax = 1 << 30;      // countdown clamp; a clamped zero is a no-op general step
 
@@ -68,6 +67,11 @@ struct RareSm {
     long long cstamp[kMaxBlock];  // step at which the cached cell was left
     long long sc1[kMaxBlock];     // completed state-1 steps
     long long since[kMaxBlock];   // first step of the current state-1 run
+    // Lane state the hot loop hands to the general step and takes back, and
+    // the lane state only the general step uses.
+    float xp[kMaxBlock], rv[kMaxBlock], F[kMaxBlock], lo[kMaxBlock], hi[kMaxBlock], c1[kMaxBlock];
+    uint32_t thi[kMaxBlock], traj[kMaxBlock];
+    int32_t left[kMaxBlock], job[kMaxBlock], cell[kMaxBlock], state[kMaxBlock], sw[kMaxBlock];
 };
 
 __device__ __forceinline__ void red_add(int64_t* p, int64_t v) {
@@ -90,13 +94,16 @@ __device__ __forceinline__ float unit_centered(uint32_t w) {
 }
 
 // Box-Muller pair scaled by sigma: k = -2 ln 2 sigma^2 (log2 is the native
-// logarithm of the special-function unit).
+// logarithm of the special-function unit).  Flush-to-zero forms: the
+// uniforms are normal numbers in (2^-24, 1) and the angle in [-pi, pi).
 __device__ __forceinline__ void noise_pair(uint32_t wa, uint32_t wb, float k, float* n0, float* n1) {
-    const float t = fmaxf(__log2f(unit_open(wa)) * k, 0.0f);
-    float r;
+    float lg, r, sn, cs;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(lg) : "f"(unit_open(wa)));
+    const float t = fmaxf(lg * k, 0.0f);
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(t));
-    float sn, cs;
-    __sincosf(6.28318530717958647692f * unit_centered(wb), &sn, &cs);
+    const float a = 6.28318530717958647692f * unit_centered(wb);
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(sn) : "f"(a));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cs) : "f"(a));
     *n0 = r * cs;
     *n1 = r * sn;
 }
@@ -139,7 +146,21 @@ __device__ __forceinline__ float force_of(const JobF& J, float xp, int st) {
 
 // Open band (lo, hi) of consecutive breakpoints around xp; lo = hi = xp when
 // xp sits on a breakpoint, so that the next step takes the general path.
+// Single barrier: the breakpoints are -L/2, -w, 0, w (clamped to the cell).
+template <bool DBL>
 __device__ __forceinline__ void band_of(const JobF& J, float xp, float* lo, float* hi) {
+    if (!DBL) {
+        const float w = J.w, hL = J.halfL, a = fabsf(xp);
+        float l, h;
+        if (a < w) { l = (xp > 0.0f) ? 0.0f : -w; h = (xp > 0.0f) ? w : 0.0f; }
+        else { l = (xp > 0.0f) ? w : -hL; h = (xp > 0.0f) ? hL : -w; }
+        l = fmaxf(l, -hL);
+        h = fminf(h, hL);
+        if (a == w || xp == 0.0f || xp == -hL) l = h = xp;
+        *lo = l;
+        *hi = h;
+        return;
+    }
     float l = -__int_as_float(0x7f800000), h = __int_as_float(0x7f800000);
     for (int i = 0; i < J.nbp; ++i) {
         const float b = J.bp[i];
@@ -305,90 +326,53 @@ __device__ __forceinline__ float one_minus_exp(float x) {
     return 1.0f - expf(x);
 }
 
-}  // namespace
+// End of a trajectory after step `done` (v: velocity after that step).
+template <bool OVER>
+__device__ __forceinline__ void retire_lane(const JobF& J, unsigned long long* retired, RareSm& sm, int t,
+                                            uint64_t done, float xp, float v, uint32_t flags) {
+    const int state = sm.state[t];
+    const int64_t sc1 = sm.sc1[t] + (state ? (int64_t)done + 1 - sm.since[t] : 0);
+    if (J.fp_mode && !(flags & LDP_FLAG_NONFINITE) && !(sm.bits[t] & B_HAS_FPT2)) flags |= LDP_FLAG_CENSORED;
+    f_retire(&J, retired, sm.traj[t], done, sc1, sm.cell[t], xp, OVER ? 0.0f : v, state, flags);
+}
 
+// The general step s of one lane (position already advanced, flip word fw):
+// the FP64 step order of ldp_fp64.cu from the index update on.  Out of line,
+// on the lane state in shared memory, so that the hot loop's registers do
+// not carry its working set.
 template <bool DBL, bool OVER>
-__global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev q, const SlotsDev S,
-                                                                 uint32_t pair_budget) {
-    __shared__ RareSm sm;
-    const int t = threadIdx.x;
-    const int64_t slot = (int64_t)blockIdx.x * blockDim.x + t;
-    const unsigned lane = t & 31u;
+__device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, RareSm* smp, int t, int64_t slot,
+                                          uint64_t s, uint32_t fw) {
+    RareSm& sm = *smp;
+    const SlotsDev& S = *Sp;
     const float kInf = __int_as_float(0x7f800000);
+    int job = sm.job[t];
+    if (job < 0) return;
+    const JobF& J = jobs[job];
+    const uint32_t traj = sm.traj[t];
+    float xp = sm.xp[t];
+    const float rv = sm.rv[t];
+    float lo = sm.lo[t], hi = sm.hi[t];
+    int cell = sm.cell[t], state = sm.state[t], sw = sm.sw[t];
+    int left = sm.left[t];
 
-    // ---- slot state ----
-    int job = (slot < S.nslots) ? S.job[slot] : -1;
-    uint32_t traj = 0;
-    uint64_t j = 0;                 // next pair: steps 2j+1, 2j+2
-    float xp = 0.f, rv = 0.f, F = 0.f, lo = -kInf, hi = kInf;
-    uint32_t thi = 0;
-    int cell = 0, state = 0, sw = 0, left = kLeftMax;
-    float c1 = 0.f, c2 = 0.f, c3 = 0.f, kn = 0.f;
-    uint32_t key0 = 0, key1 = 0;
-
-    // Per-job constants into registers; band, force and countdown from the
-    // position.  s = next step.
-    auto bind = [&](uint64_t s) {
-        const JobF& J = q.jobs[job];
-        if (OVER) c1 = J.c_drift;
-        else { c1 = J.hdt_invM; c2 = J.hdt; c3 = J.expg; }
-        kn = J.bm_k;
-        key0 = J.key0;
-        key1 = J.key1;
-        thi = thi_of(J, state);
-        band_of(J, xp, &lo, &hi);
-        F = force_of<DBL>(J, xp, state);
-        left = steps_to_special(J, s - 1, sm.nxf[t]);
-        j = (s - 1) >> 1;
-    };
-
-    if (job >= 0) {
-        const JobF& J = q.jobs[job];
-        traj = (uint32_t)S.traj[slot];
-        const uint64_t s = (uint64_t)S.step[slot];
-        xp = S.xp[slot];
-        rv = S.rv[slot];
-        cell = S.cell[slot];
-        const int st = S.st[slot];
-        state = st & 1;
-        sw = st >> 1;
-        sm.bits[t] = (uint32_t)J.bits[traj];
-        sm.init0[t] = J.init_idx0[traj];
-        sm.idx2[t] = J.idx2_0[traj];
-        sm.tpt2w[t] = J.tpt2_well[traj];
-        sm.fpt[t] = J.fpt_last[traj];
-        sm.fpt2[t] = J.fpt2_last[traj];
-        sm.tpt[t] = J.tpt_last[traj];
-        sm.tpt2[t] = J.tpt2_last[traj];
-        sm.ckey[t] = S.ckey[slot];
-        sm.cstamp[t] = S.cstamp[slot];
-        sm.sc1[t] = S.sc1[slot];
-        sm.since[t] = S.since[slot];
-        sm.cgw[t] = S.cgw[slot];
-        sm.fidx[t] = S.fidx[slot];
-        sm.nxf[t] = S.nxf[slot];
-        bind(s);
-    }
-
-    // End of a trajectory after step `done` (v: velocity after that step).
-    auto retire = [&](const JobF& J, uint64_t done, float v, uint32_t flags) {
-        const int64_t sc1 = sm.sc1[t] + (state ? (int64_t)done + 1 - sm.since[t] : 0);
-        if (J.fp_mode && !(flags & LDP_FLAG_NONFINITE) && !(sm.bits[t] & B_HAS_FPT2)) flags |= LDP_FLAG_CENSORED;
-        f_retire(&J, S.retired, traj, done, sc1, cell, xp, OVER ? 0.0f : v, state, flags);
-        job = -1;
-        lo = -kInf;
-        hi = kInf;
-        thi = 0;
-        F = 0.f;
-        left = kLeftMax;
+    auto retire = [&](uint64_t done, float v, uint32_t flags) {
+        sm.cell[t] = cell;
+        sm.state[t] = state;
+        retire_lane<OVER>(J, S.retired, sm, t, done, xp, v, flags);
+        sm.job[t] = -1;
+        sm.lo[t] = -kInf;
+        sm.hi[t] = kInf;
+        sm.thi[t] = 0;
+        sm.F[t] = 0.f;
+        sm.left[t] = kLeftMax;
     };
 
     // Cell (double model: local barrier) entry: write the state of the key
     // left through to the ring, take the entered key's state and stamp from
     // the one-entry cache or the ring, and catch it up over the steps it was
-    // not observed (UpdateBarrierStateEta, S.h:2025-2068 / D.h:2468-2517;
-    // probability in FP64 as in the FP64 path).
-    auto enter = [&](const JobF& J, uint64_t s, int key_prev, int st, int key_cur) -> int {
+    // not observed (UpdateBarrierStateEta, S.h:2025-2068 / D.h:2468-2517).
+    auto enter = [&](int key_prev, int st, int key_cur) -> int {
         const int64_t n = J.ntraj;
         const int rmask = S.ring_slots - 1;
         if (sw & W_EVICT) red_add(&J.counts[(int64_t)LDP_C_EVICT * n + traj], 1);
@@ -426,13 +410,14 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
     // Renewal statistics (UpdateStatistics, S.h:2334-2592 / D.h:2931-3209)
     // with integer step clocks.  Returns true when a FIRST_PASSAGE
     // trajectory ends.
-    auto events = [&](const JobF& J, int64_t now, bool dWell, bool dCell, int well) -> bool {
+    auto events = [&](int64_t now, bool dWell, bool dCell, int well) -> bool {
         const int64_t n = J.ntraj;
         int64_t* C = J.counts;
         int64_t* U = J.ssum;
         uint32_t bits = sm.bits[t];
         bool done = false;
-        if (!DBL && J.wt && !J.fp_mode) {
+        const int evm = J.evm;
+        if (!DBL && (evm & EV_WT)) {
             if (dWell) { J.wt_tick[traj] = now; bits |= B_WT_PASSED; }
             else if (dCell && (bits & B_WT_PASSED)) {
                 int64_t& nwt = C[(int64_t)LDP_C_WT * n + traj];
@@ -442,8 +427,8 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
                 bits &= ~B_WT_PASSED;
             }
         }
-        if (J.fpt || J.fp_mode) {
-            if (!DBL && !J.fp_mode) {
+        if (evm & EV_FPT2) {
+            if (!DBL && (evm & EV_FPT)) {
                 if ((bits & B_FPT_UP) && dCell) {
                     // initial barrier pair (S.h:2364-2388)
                     bits &= ~(B_FPT_UP | B_INIT0 | B_INIT1);
@@ -478,10 +463,10 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
                 red_add(&C[(int64_t)LDP_C_FPT2 * n + traj], 1);
                 sm.fpt2[t] = now;
                 sm.idx2[t] = (well == cell) ? cell : cell - 1;
-                if (J.fp_mode) done = true;
+                if (evm & EV_FP) done = true;
             }
         }
-        if (!DBL && J.tpt && !J.fp_mode) {
+        if (!DBL && (evm & EV_TPT)) {
             if (dCell) { bits &= ~B_TPT_UP; sm.tpt[t] = now; }
             if (!(bits & B_TPT_UP) && dWell) {
                 bits |= B_TPT_UP;
@@ -504,7 +489,7 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
         }
         // An FPTCG evaluation at the well of the previous one changes nothing
         // (every entry it hits already holds that well), so it is skipped.
-        if (J.cg && !J.fp_mode && dCell && well != sm.cgw[t]) {
+        if ((evm & EV_CG) && dCell && well != sm.cgw[t]) {
             sm.cgw[t] = well;
             for (int jj = 0; jj < J.n_cg; ++jj) {
                 if (cg_hit32(well, J.cg_size[jj])) {
@@ -526,89 +511,187 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
         return done;
     };
 
-    // The general step s (position already advanced with flip word fw):
-    // the FP64 step order of ldp_fp64.cu from the index update on.
-    auto general = [&](uint64_t s, uint32_t fw) {
-        if (job < 0) return;
-        const JobF& J = q.jobs[job];
-        if (!(fabsf(xp) < kInf)) {
-            retire(J, s - 1, rv, LDP_FLAG_NONFINITE);
-            return;
+    if (xp > lo && xp < hi && fw > sm.thi[t]) {
+        // Only the countdown ran out: a frame and/or the last step.
+        const float F = sm.F[t];
+        const float vk = OVER ? 0.0f : fmaf(F, sm.c1[t], rv);
+        if ((long long)s == sm.nxf[t]) {
+            f_record<DBL>(J, traj, sm.fidx[t], cell, xp, vk, F, state);
+            sm.fidx[t] += 1;
+            sm.nxf[t] += (long long)J.freq_save;
         }
-        const int cell_prev = cell;
-        const int lb_prev = sw & W_LB;
-        const int well_prev = cell_prev - (lo < 0.0f ? 1 : 0);
-        const bool moved = !(xp > lo && xp < hi);
-        if (moved) {
+        sm.left[t] = steps_to_special(J, s, sm.nxf[t]);
+        if (s == J.nsteps) retire(s, vk, 0);
+        return;
+    }
+    if (!(fabsf(xp) < kInf)) {
+        retire(s - 1, rv, LDP_FLAG_NONFINITE);
+        return;
+    }
+    const int cell_prev = cell;
+    const int lb_prev = sw & W_LB;
+    const int well_prev = cell_prev - (lo < 0.0f ? 1 : 0);
+    const bool moved = !(xp > lo && xp < hi);
+    if (moved) {
+        if (xp >= J.halfL) { xp -= J.L; ++cell; }
+        else if (xp < -J.halfL) { xp += J.L; --cell; }
+        if (!(xp >= -J.halfL && xp < J.halfL)) {
+            // more than one cell in one step
+            const float k = floorf(xp * J.invLf + 0.5f);
+            xp = fmaf(-k, J.L, xp);
+            cell += (int)k;
             if (xp >= J.halfL) { xp -= J.L; ++cell; }
             else if (xp < -J.halfL) { xp += J.L; --cell; }
-            if (!(xp >= -J.halfL && xp < J.halfL)) {
-                // more than one cell in one step
-                const float k = floorf(xp * J.invLf + 0.5f);
-                xp = fmaf(-k, J.L, xp);
-                cell += (int)k;
-                if (xp >= J.halfL) { xp -= J.L; ++cell; }
-                else if (xp < -J.halfL) { xp += J.L; --cell; }
-            }
         }
-        const int well = cell - (xp < 0.0f ? 1 : 0);
-        const int lb = DBL ? (xp < J.xc ? 0 : 1) : 0;
-        const bool dCell = cell != cell_prev;
-        const bool dWell = well != well_prev;
-        const bool dKey = DBL ? (lb != lb_prev) : dCell;
-        int st = state;
-        if (fw <= thi) {
-            bool flip = fw < thi;
-            if (fw == thi) {
-                const uint64_t T = J.eq ? J.T_eq : J.T_as[st];
-                flip = philox_at(s, traj, TAG_REFINE, J.key0, J.key1).w0 < (uint32_t)T;
-            }
-            st ^= (int)flip;
+    }
+    const int well = cell - (xp < 0.0f ? 1 : 0);
+    const int lb = DBL ? (xp < J.xc ? 0 : 1) : 0;
+    const bool dCell = cell != cell_prev;
+    const bool dWell = well != well_prev;
+    const bool dKey = DBL ? (lb != lb_prev) : dCell;
+    uint32_t thi = sm.thi[t];
+    int st = state;
+    if (fw <= thi) {
+        bool flip = fw < thi;
+        if (fw == thi) {
+            const uint64_t T = J.eq ? J.T_eq : J.T_as[st];
+            flip = philox_at(s, traj, TAG_REFINE, J.key0, J.key1).w0 < (uint32_t)T;
         }
-        if (dKey) st = enter(J, s, fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb));
-        if (DBL) sw = (sw & ~W_LB) | (lb ? W_LB : 0);
-        if (st != state) {
-            if (st) sm.since[t] = (long long)s;
-            else sm.sc1[t] += (long long)s - sm.since[t];
-            state = st;
-            thi = thi_of(J, st);
+        st ^= (int)flip;
+    }
+    if (dKey) st = enter(fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb));
+    if (DBL) sw = (sw & ~W_LB) | (lb ? W_LB : 0);
+    if (st != state) {
+        if (st) sm.since[t] = (long long)s;
+        else sm.sc1[t] += (long long)s - sm.since[t];
+        state = st;
+        thi = thi_of(J, st);
+    }
+    band_of<DBL>(J, xp, &lo, &hi);
+    const float F = force_of<DBL>(J, xp, state);
+    bool finish = false;
+    if (dCell || dWell) finish = events((int64_t)s, dWell, dCell, well);
+    const float vk = OVER ? 0.0f : fmaf(F, sm.c1[t], rv);
+    if (left == 0) {
+        if ((long long)s == sm.nxf[t]) {
+            f_record<DBL>(J, traj, sm.fidx[t], cell, xp, vk, F, state);
+            sm.fidx[t] += 1;
+            sm.nxf[t] += (long long)J.freq_save;
         }
-        band_of(J, xp, &lo, &hi);
+        if (s == J.nsteps) finish = true;
+        left = steps_to_special(J, s, sm.nxf[t]);
+    }
+    sm.xp[t] = xp;
+    sm.cell[t] = cell;
+    sm.state[t] = state;
+    sm.sw[t] = sw;
+    sm.lo[t] = lo;
+    sm.hi[t] = hi;
+    sm.thi[t] = thi;
+    sm.F[t] = F;
+    sm.left[t] = left;
+    if (finish) retire(s, vk, 0);
+}
+
+}  // namespace
+
+#ifndef LDP_FP32_MIN_BLOCKS
+// Resident 256-thread blocks per SM the register budget is sized for: 3
+// gives the hot loop 80 registers without spills (measured faster than 4
+// blocks at 64 registers, which spill in the loop).
+#define LDP_FP32_MIN_BLOCKS 3
+#endif
+
+template <bool DBL, bool OVER>
+__global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kernel(
+    const __grid_constant__ QueueDev q, const __grid_constant__ SlotsDev S, uint32_t pair_budget) {
+    __shared__ RareSm sm;
+    const int t = threadIdx.x;
+    const int64_t slot = (int64_t)blockIdx.x * blockDim.x + t;
+    const unsigned lane = t & 31u;
+    const float kInf = __int_as_float(0x7f800000);
+
+    // ---- hot lane state (registers); the rest lives in sm ----
+    int job = (slot < S.nslots) ? S.job[slot] : -1;
+    uint32_t traj = 0;
+    uint64_t j = 0;                 // next pair: steps 2j+1, 2j+2
+    float xp = 0.f, rv = 0.f, F = 0.f, lo = -kInf, hi = kInf;
+    uint32_t thi = 0;
+    int left = kLeftMax;
+    float c1 = 0.f, c2 = 0.f, c3 = 0.f, kn = 0.f;
+    uint32_t key0 = 0, key1 = 0;
+    sm.job[t] = job;
+
+    // Per-job constants into registers; band, force and countdown from the
+    // position.  s = next step.
+    auto bind = [&](uint64_t s) {
+        const JobF& J = q.jobs[job];
+        if (OVER) c1 = J.c_drift;
+        else { c1 = J.hdt_invM; c2 = J.hdt; c3 = J.expg; }
+        sm.c1[t] = c1;
+        sm.traj[t] = traj;
+        kn = J.bm_k;
+        key0 = J.key0;
+        key1 = J.key1;
+        const int state = sm.state[t];
+        thi = thi_of(J, state);
+        band_of<DBL>(J, xp, &lo, &hi);
         F = force_of<DBL>(J, xp, state);
-        bool finish = false;
-        if (dCell || dWell) finish = events(J, (int64_t)s, dWell, dCell, well);
-        const float vk = OVER ? 0.0f : fmaf(F, c1, rv);
-        if (left == 0) {
-            if ((long long)s == sm.nxf[t]) {
-                f_record<DBL>(J, traj, sm.fidx[t], cell, xp, vk, F, state);
-                sm.fidx[t] += 1;
-                sm.nxf[t] += (long long)J.freq_save;
-            }
-            if (s == J.nsteps) finish = true;
-            left = steps_to_special(J, s, sm.nxf[t]);
-        }
-        if (finish) retire(J, s, vk, 0);
+        left = steps_to_special(J, s - 1, sm.nxf[t]);
+        j = (s - 1) >> 1;
     };
+
+    if (job >= 0) {
+        const JobF& J = q.jobs[job];
+        traj = (uint32_t)S.traj[slot];
+        const uint64_t s = (uint64_t)S.step[slot];
+        xp = S.xp[slot];
+        rv = S.rv[slot];
+        sm.cell[t] = S.cell[slot];
+        const int st = S.st[slot];
+        sm.state[t] = st & 1;
+        sm.sw[t] = st >> 1;
+        sm.bits[t] = (uint32_t)J.bits[traj];
+        sm.init0[t] = J.init_idx0[traj];
+        sm.idx2[t] = J.idx2_0[traj];
+        sm.tpt2w[t] = J.tpt2_well[traj];
+        sm.fpt[t] = J.fpt_last[traj];
+        sm.fpt2[t] = J.fpt2_last[traj];
+        sm.tpt[t] = J.tpt_last[traj];
+        sm.tpt2[t] = J.tpt2_last[traj];
+        sm.ckey[t] = S.ckey[slot];
+        sm.cstamp[t] = S.cstamp[slot];
+        sm.sc1[t] = S.sc1[slot];
+        sm.since[t] = S.since[slot];
+        sm.cgw[t] = S.cgw[slot];
+        sm.fidx[t] = S.fidx[slot];
+        sm.nxf[t] = S.nxf[slot];
+        bind(s);
+    }
 
     bool dry = false;   // the queue had nothing left for this warp
     for (uint32_t it = 0; it < pair_budget; ++it) {
         // ---- warp-aggregated refill of idle lanes ----
         const unsigned idle = __ballot_sync(kFull, job < 0);
-        if (idle) {
+        if (__builtin_expect(idle != 0, 0)) {
             const bool need = job < 0 && !dry && slot < S.nslots;
             const unsigned m = __ballot_sync(kFull, need);
             if (m) {
                 const int leader = __ffs(m) - 1;
                 unsigned long long base = 0, got = 0;
                 if ((int)lane == leader) {
+                    // One fetch-and-add per warp.  A claim that runs past the
+                    // tail gets the part below it; the overshoot of head is
+                    // clamped back to the tail when more work is published
+                    // (fp32_publish_kernel, stream-ordered between launches).
                     const unsigned long long tail = *(volatile unsigned long long*)q.tail;
-                    unsigned long long old = *(volatile unsigned long long*)q.head;
-                    for (int tries = 0; tries < kClaimTries; ++tries) {
-                        if (old >= tail) break;
-                        const unsigned long long want = min((unsigned long long)__popc(m), tail - old);
-                        const unsigned long long prev = atomicCAS(q.head, old, old + want);
-                        if (prev == old) { base = old; got = want; break; }
-                        old = prev;
+                    if (*(volatile unsigned long long*)q.head < tail) {
+                        const unsigned long long want = (unsigned long long)__popc(m);
+                        const unsigned long long old = atomicAdd(q.head, want);
+                        if (old < tail) {
+                            base = old;
+                            got = min(want, tail - old);
+                        }
                     }
                 }
                 base = __shfl_sync(kFull, base, leader);
@@ -620,10 +703,20 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
                         traj = (uint32_t)f_resolve(q.range_end, q.range_job, q.range_first, q.nranges,
                                                    (int64_t)(base + rank), &job);
                         const JobF* Jn = &q.jobs[job];
-                        f_start<DBL, OVER>(Jn, S.ring, S.nslots, S.ring_slots, slot, traj, &sm, t, &xp, &rv, &cell,
-                                           &state, &sw);
+                        f_start<DBL, OVER>(Jn, S.ring, S.nslots, S.ring_slots, slot, traj, &sm, t, &xp, &rv,
+                                           &sm.cell[t], &sm.state[t], &sm.sw[t]);
+                        sm.job[t] = job;
                         bind(1);
-                        if (Jn->nsteps == 0) retire(*Jn, 0, rv, 0);
+                        if (Jn->nsteps == 0) {
+                            retire_lane<OVER>(*Jn, S.retired, sm, t, 0, xp, rv, 0);
+                            job = -1;
+                            sm.job[t] = -1;
+                            lo = -kInf;
+                            hi = kInf;
+                            thi = 0;
+                            F = 0.f;
+                            left = kLeftMax;
+                        }
                     }
                 }
             }
@@ -635,10 +728,9 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
         }
 
         // ---- one Philox block, two steps ----
-        const Words w = philox((uint32_t)j, (uint32_t)(j >> 32), traj, TAG_STEP, key0, key1);
+        const Words w = philox_wide((uint32_t)j, (uint32_t)(j >> 32), traj, TAG_STEP, key0, key1);
         float n0, n1;
         noise_pair(w.w0, w.w1, kn, &n0, &n1);
-        const uint64_t s0 = 2 * j + 1;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const float nz = h ? n1 : n0;
@@ -655,7 +747,22 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
                 xp = fmaf(rv, c2, xp);
             }
             --left;
-            if (!(xp > lo && xp < hi) || fw <= thi || left == 0) general(s0 + h, fw);
+            if (__builtin_expect(!(xp > lo && xp < hi) || fw <= thi || left == 0, 0)) {
+                sm.xp[t] = xp;
+                sm.rv[t] = rv;
+                sm.left[t] = left;
+                sm.lo[t] = lo;
+                sm.hi[t] = hi;
+                sm.thi[t] = thi;
+                general_step<DBL, OVER>(q.jobs, &S, &sm, t, slot, 2 * j + 1 + h, fw);
+                xp = sm.xp[t];
+                F = sm.F[t];
+                lo = sm.lo[t];
+                hi = sm.hi[t];
+                thi = sm.thi[t];
+                left = sm.left[t];
+                job = sm.job[t];
+            }
             if (!OVER) rv = fmaf(F, c1, rv);
         }
         ++j;
@@ -669,8 +776,8 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
         S.step[slot] = (int64_t)(2 * j + 1);
         S.xp[slot] = xp;
         S.rv[slot] = rv;
-        S.cell[slot] = cell;
-        S.st[slot] = state | (sw << 1);
+        S.cell[slot] = sm.cell[t];
+        S.st[slot] = sm.state[t] | (sm.sw[t] << 1);
         S.ckey[slot] = sm.ckey[t];
         S.cstamp[slot] = sm.cstamp[t];
         S.sc1[slot] = sm.sc1[t];
@@ -689,9 +796,35 @@ __global__ void __launch_bounds__(256, 4) fp32_persistent_kernel(const QueueDev 
     }
 }
 
+// Publishes item ranges [.., new_tail): clamps the head (claims may have run
+// past the old tail) and moves the tail; one thread, between launches.
+__global__ void fp32_publish_kernel(unsigned long long* head, unsigned long long* tail, int32_t* nranges,
+                                    unsigned long long new_tail, int32_t new_nranges) {
+    const unsigned long long t = *tail;
+    if (*head > t) *head = t;
+    *tail = new_tail;
+    *nranges = new_nranges;
+}
+
+int launch_fp32_publish(const QueueDev& q, unsigned long long new_tail, int32_t new_nranges, void* stream) {
+    fp32_publish_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(q.head, q.tail, q.nranges, new_tail, new_nranges);
+    return (int)cudaGetLastError();
+}
+
+template <bool DBL, bool OVER>
+static cudaError_t fp32_kernel_attrs() {
+    // The kernel reads little global memory: give shared memory the whole
+    // carveout so that the occupancy the grid is sized for is resident.
+    return cudaFuncSetAttribute(fp32_persistent_kernel<DBL, OVER>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared);
+}
+
 int fp32_blocks_per_sm(bool dbl, bool over, int block) {
     int n = 0;
     cudaError_t e;
+    if (dbl) e = over ? fp32_kernel_attrs<true, true>() : fp32_kernel_attrs<true, false>();
+    else e = over ? fp32_kernel_attrs<false, true>() : fp32_kernel_attrs<false, false>();
+    if (e != cudaSuccess) return 0;
     if (dbl) e = over ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp32_persistent_kernel<true, true>, block, 0)
                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp32_persistent_kernel<true, false>, block, 0);
     else e = over ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp32_persistent_kernel<false, true>, block, 0)

@@ -19,11 +19,22 @@ namespace ldp {
 constexpr int kFp32MaxJobs = 16384;     // resident jobs per queue
 constexpr int kFp32MaxRanges = 1 << 20; // published item ranges per queue (one per job)
 
+// Statistics switches of a job, folded for the kernel's event path.
+enum : int32_t {
+    EV_WT = 1,     // waiting times (single barrier, fixed steps)
+    EV_FPT = 2,    // bottom-to-top first passages (single barrier, fixed steps)
+    EV_FPT2 = 4,   // bottom-to-bottom first passages (FPT on, or FIRST_PASSAGE mode)
+    EV_TPT = 8,    // transition paths (single barrier, fixed steps)
+    EV_CG = 16,    // coarse-grained first passages (fixed steps)
+    EV_FP = 32     // FIRST_PASSAGE mode: the first FPT2 event ends the trajectory
+};
+
 // Per-job constants and output pointers (device resident, one per job).
 struct JobF {
     // model switches (jobs of one queue share dbl/over)
     int32_t eta, eq, rs, rv, us, init_state, wt, fpt, tpt, cg, n_cg, write_x, at_bottom, fp_mode;
-    int32_t lanes, nruns, slots_log2, pad0;
+    int32_t lanes, nruns, slots_log2;
+    int32_t evm;         // EV_* statistics switches of the event path
     int32_t cg_size[LDP_MAX_CG];
     uint32_t key0, key1;
     // FP32 step constants
@@ -87,6 +98,8 @@ struct SlotsDev {
     int32_t ring_slots;
 };
 
+// Appends published work: clamps head to the old tail, sets tail and nranges.
+int launch_fp32_publish(const QueueDev& q, unsigned long long new_tail, int32_t new_nranges, void* stream);
 // Resident blocks per SM of the persistent kernel (0 on error).
 int fp32_blocks_per_sm(bool dbl, bool over, int block);
 int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint32_t pair_budget,

@@ -118,6 +118,12 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
     J->eta = k.eta; J->eq = k.eq; J->rs = k.rs; J->rv = k.rv; J->us = k.us; J->init_state = k.init_state;
     J->wt = k.wt; J->fpt = k.fpt; J->tpt = k.tpt; J->cg = k.cg; J->n_cg = k.n_cg; J->write_x = k.write_x;
     J->at_bottom = k.at_bottom; J->fp_mode = k.fp_mode; J->lanes = k.lanes; J->nruns = k.nruns;
+    {
+        const bool fp = k.fp_mode != 0, single = !k.dbl;
+        J->evm = ((single && k.wt && !fp) ? EV_WT : 0) | ((single && k.fpt && !fp) ? EV_FPT : 0) |
+                 ((k.fpt || fp) ? EV_FPT2 : 0) | ((single && k.tpt && !fp) ? EV_TPT : 0) |
+                 ((k.cg && !fp) ? EV_CG : 0) | (fp ? EV_FP : 0);
+    }
     for (int j = 0; j < LDP_MAX_CG; ++j) J->cg_size[j] = k.cg_size[j] ? k.cg_size[j] : 1;
     J->key0 = k.key0; J->key1 = k.key1;
     J->L = k.fL; J->halfL = k.fhalfL; J->w = k.fw;
@@ -226,14 +232,13 @@ int fp32_register(ldp_job* job) {
     Q.h_stage[1] = (int64_t)Q.tail;       // range_end
     Q.h_stage[2] = 0;                      // range_first
     Q.h_stage[3] = slot;                   // range_job (low 32 bits)
-    Q.h_stage[4] = r + 1;                  // nranges
-    Q.h_stage[5] = (int64_t)Q.tail;        // tail
     cudaMemcpyAsync(&Q.q.range_end[r], &Q.h_stage[1], sizeof(int64_t), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(&Q.q.range_first[r], &Q.h_stage[2], sizeof(int64_t), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(&Q.q.range_job[r], &Q.h_stage[3], sizeof(int32_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(Q.q.nranges, &Q.h_stage[4], sizeof(int32_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(Q.q.tail, &Q.h_stage[5], sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
     Q.nranges = r + 1;
+    e = launch_fp32_publish(Q.q, Q.tail, (int32_t)Q.nranges, st);
+    if (e) return e;
+    ++job->launches;
     return (int)cudaGetLastError();
 }
 

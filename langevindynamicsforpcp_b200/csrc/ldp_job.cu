@@ -692,13 +692,13 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
             ldp_set_error(ctx, "cudaMalloc of %zu bytes failed", job_arena(job, false));
             return LDP_ERR_NOMEM;
         }
+        job->launches = 0;
         int e = fp32_register(job);
         if (e) {
             ldp_set_error(ctx, "FP32 registration failed: %s", cudaGetErrorString((cudaError_t)e));
             return LDP_ERR_DEVICE;
         }
         job->submitted = true;
-        job->launches = 0;
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[0], s));
         const int t = job->fp32_type;
         launches[t] += fp32_estimate_launches(job);

@@ -730,18 +730,35 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
     return 0;
 }
 
+/* Per-trajectory mean-square displacement at each lag
+ * (MeanSquareDisplacementBruteForce, src/langevinDynamicsSingleBarrier.h:24-45):
+ * msd0 = sum over origins k < nframe - lag of (x[k + lag] - x[k])^2, divided
+ * by the origin count.  The sum is taken in a fixed order that a warp of 32
+ * lanes evaluates without shared-memory bank conflicts: 32 partial sums
+ * p[l] over the origins k = l, l + 32, l + 64, ... (each in increasing k),
+ * then the tree p[l] += p[l + h] for l < h, h = 16, 8, 4, 2, 1, whose result
+ * is p[0].  It differs from the reference's single running sum only in
+ * rounding. */
 void ldpo_msd_traj(const double *frames, int64_t nframe, int64_t ntraj, const int64_t *lags, int64_t nlag,
                    double *msd0) {
     for (int64_t g = 0; g < ntraj; ++g) {
         for (int64_t ii = 0; ii < nlag; ++ii) {
-            int64_t lag = lags[ii];
+            const int64_t lag = lags[ii];
+            const int64_t cnt = nframe - lag;
             double acc = 0.0;
-            if (nframe - lag > 0) {
-                for (int64_t kk = 0; kk < nframe - lag; ++kk) {
-                    double d = frames[(kk + lag) * ntraj + g] - frames[kk * ntraj + g];
-                    acc += d * d;
+            if (cnt > 0) {
+                double p[32];
+                for (int l = 0; l < 32; ++l) {
+                    double a = 0.0;
+                    for (int64_t kk = l; kk < cnt; kk += 32) {
+                        const double d = frames[(kk + lag) * ntraj + g] - frames[kk * ntraj + g];
+                        a = a + d * d;
+                    }
+                    p[l] = a;
                 }
-                acc /= (double)(nframe - lag);
+                for (int h = 16; h >= 1; h >>= 1)
+                    for (int l = 0; l < h; ++l) p[l] = p[l] + p[l + h];
+                acc = p[0] / (double)cnt;
             }
             msd0[ii * ntraj + g] = acc;
         }

@@ -47,7 +47,8 @@ int64_t  ldpo_lags(const ldp_params *p, int64_t *lags, int64_t cap);
 int      ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out);
 
 /* Per-trajectory MSD (MeanSquareDisplacementBruteForce, S.h:24-45):
- * frames [nframe][ntraj], msd0 [nlag][ntraj]. */
+ * frames [nframe][ntraj], msd0 [nlag][ntraj].  Origins are summed as 32
+ * interleaved partial sums combined by a fixed tree (see the definition). */
 void     ldpo_msd_traj(const double *frames, int64_t nframe, int64_t ntraj,
                        const int64_t *lags, int64_t nlag, double *msd0);
 
