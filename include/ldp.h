@@ -175,6 +175,7 @@ typedef struct ldp_job_info {
     int32_t precision;
     int32_t mode;
     int32_t done;
+    int64_t device_bytes; /* device memory the job holds while it runs      */
 } ldp_job_info;
 
 /*
@@ -257,11 +258,54 @@ ldp_status  ldp_submit(ldp_ctx *ctx, ldp_job *job);   /* asynchronous      */
  * work queue before any launch, so their trajectories share every persistent
  * launch (the reference runs one .inp per mpirun; no counterpart). */
 ldp_status  ldp_submit_batch(ldp_ctx *ctx, ldp_job **jobs, int njobs);
+/* As ldp_submit_batch for FP32 batched jobs only, with every persistent
+ * launch and every job's post-processing captured in one CUDA graph (launch
+ * count: an upper bound that drains the queues), so the host is not involved
+ * until the results.  The batch's device time is in the first job's timing.
+ * A parameter scan runs as one graph launch (no counterpart in the
+ * reference, which runs one .inp per process). */
+ldp_status  ldp_submit_batch_graph(ldp_ctx *ctx, ldp_job **jobs, int njobs);
 ldp_status  ldp_poll(ldp_ctx *ctx, ldp_job *job, int *done);
 ldp_status  ldp_wait(ldp_ctx *ctx, ldp_job *job);
 ldp_status  ldp_job_info_get(const ldp_job *job, ldp_job_info *info);
 ldp_status  ldp_job_timing_get(const ldp_job *job, ldp_timing *t);
 void        ldp_job_destroy(ldp_job *job);
+
+/* Serving loop (continuous batching of FP32 batched jobs).  No counterpart
+ * in the reference, which runs one .inp per MPI process (src/mpiKernel.cpp).
+ * Requests are submitted at any time (ldp_server_submit is thread-safe);
+ * each ldp_server_step admits queued jobs in arrival order while their
+ * device footprint fits hbm_budget, keeps short persistent launches in
+ * flight for every model type with work, and finishes jobs whose
+ * trajectories all retired.  Jobs joining mid-run share the launches with
+ * those already running; every result equals that of the job run alone.
+ * Drive it with ldp_server_step from one thread (the one that owns ctx). */
+typedef struct ldp_server ldp_server;
+typedef enum {
+    LDP_SRV_QUEUED = 0, LDP_SRV_RUNNING = 1, LDP_SRV_FINISHING = 2, LDP_SRV_DONE = 3, LDP_SRV_FAILED = 4
+} ldp_server_state;
+typedef struct ldp_server_opts {
+    int64_t hbm_budget;     /* bytes of job arenas resident at once (0: 80% of free memory) */
+    int64_t pair_budget;    /* step pairs per slot per persistent launch (0: 2048)           */
+    int32_t max_inflight;   /* persistent launches in flight per model type (1..16)         */
+    int32_t pad;
+} ldp_server_opts;
+typedef struct ldp_server_info {
+    int64_t queued, running, finishing, done;
+    int64_t hbm_in_use, hbm_budget;
+    int64_t launches;
+} ldp_server_info;
+void        ldp_server_opts_default(ldp_server_opts *o);
+ldp_status  ldp_server_create(ldp_ctx *ctx, const ldp_server_opts *o, ldp_server **out);
+ldp_status  ldp_server_submit(ldp_server *s, const ldp_params *p, const ldp_job_opts *o, uint64_t *ticket);
+ldp_status  ldp_server_step(ldp_server *s, int *ndone);
+/* state: ldp_server_state; latency_s: submission to done (0 until done). */
+ldp_status  ldp_server_poll(ldp_server *s, uint64_t ticket, int *state, double *latency_s);
+/* The finished job (owned by the server until ldp_server_release). */
+ldp_status  ldp_server_job(ldp_server *s, uint64_t ticket, ldp_job **job);
+ldp_status  ldp_server_release(ldp_server *s, uint64_t ticket);
+ldp_status  ldp_server_info_get(ldp_server *s, ldp_server_info *info);
+void        ldp_server_destroy(ldp_server *s);
 
 /* Results.  Replaces the getters GetFirstPassageTimeAverage{,2},
  * GetTransitionPathTimeAverage{,2}, GetFirstPassageTimeCGAverage2,

@@ -101,6 +101,16 @@ class Job:
         _check(L.lib().ldp_job_create(ctx.handle, C.byref(params), C.byref(o), C.byref(h)), ctx)
         self.handle = h
 
+    @classmethod
+    def borrowed(cls, ctx: Context, handle) -> "Job":
+        """A view of a job owned elsewhere (a serving loop): results only;
+        close() does not destroy it."""
+        j = cls.__new__(cls)
+        j.ctx, j.opts, j.params = ctx, None, None
+        j.handle = C.c_void_p(handle.value if isinstance(handle, C.c_void_p) else handle)
+        j._borrowed = True
+        return j
+
     # -- execution ---------------------------------------------------------
     def submit(self) -> "Job":
         _check(L.lib().ldp_submit(self.ctx.handle, self.handle), self.ctx)
@@ -181,9 +191,9 @@ class Job:
         _check(L.lib().ldp_job_write_outputs(self.handle, directory.encode()), self.ctx)
 
     def close(self):
-        if self.handle:
+        if self.handle and not getattr(self, "_borrowed", False):
             L.lib().ldp_job_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __enter__(self):
         return self
@@ -192,11 +202,14 @@ class Job:
         self.close()
 
 
-def submit_batch(ctx: Context, jobs) -> None:
+def submit_batch(ctx: Context, jobs, graph: bool = False) -> None:
     """Submits several jobs together (ldp_submit_batch): FP32 batched jobs
-    share every persistent launch."""
+    share every persistent launch.  graph=True (FP32 batched jobs only) runs
+    all launches and post-processing as one CUDA graph
+    (ldp_submit_batch_graph)."""
     arr = (C.c_void_p * len(jobs))(*[j.handle for j in jobs])
-    _check(L.lib().ldp_submit_batch(ctx.handle, arr, len(jobs)), ctx)
+    fn = L.lib().ldp_submit_batch_graph if graph else L.lib().ldp_submit_batch
+    _check(fn(ctx.handle, arr, len(jobs)), ctx)
 
 
 def _ctx_mark(self, mark: int) -> None:

@@ -75,7 +75,7 @@ class JobOpts(C.Structure):
 class JobInfo(C.Structure):
     _fields_ = [("ntraj", C.c_int64), ("nframe", C.c_int64), ("nlag", C.c_int64), ("steps", C.c_int64),
                 ("tick_cap", C.c_int64), ("n_cg", C.c_int32), ("precision", C.c_int32), ("mode", C.c_int32),
-                ("done", C.c_int32)]
+                ("done", C.c_int32), ("device_bytes", C.c_int64)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -88,6 +88,19 @@ class TrajResults(C.Structure):
                 ("v_final", _DP), ("state_final", _I32P), ("ticks", _I64P), ("frames_x", _DP),
                 ("frames_v", _DP), ("frames_f", _DP), ("frames_barrier", _DP), ("frames_pe", _DP),
                 ("frames_ke", _DP), ("frames_state", _DP)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget", C.c_int64), ("pair_budget", C.c_int64), ("max_inflight", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("queued", C.c_int64), ("running", C.c_int64), ("finishing", C.c_int64), ("done", C.c_int64),
+                ("hbm_in_use", C.c_int64), ("hbm_budget", C.c_int64), ("launches", C.c_int64)]
+
+
+SRV_QUEUED, SRV_RUNNING, SRV_FINISHING, SRV_DONE, SRV_FAILED = range(5)
 
 
 class Timing(C.Structure):
@@ -115,6 +128,7 @@ SIGNATURES = {
     "ldp_job_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "ldp_submit": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ldp_submit_batch": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]),
+    "ldp_submit_batch_graph": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]),
     "ldp_ctx_mark": (C.c_int, [C.c_void_p, C.c_int]),
     "ldp_ctx_elapsed_ms": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "ldp_ctx_synchronize": (C.c_int, [C.c_void_p]),
@@ -128,6 +142,15 @@ SIGNATURES = {
     "ldp_job_msd_traj": (C.c_int, [C.c_void_p, _DP]),
     "ldp_job_write_outputs": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ldp_run_inp": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(JobOpts), C.c_char_p]),
+    "ldp_server_opts_default": (None, [C.POINTER(ServerOpts)]),
+    "ldp_server_create": (C.c_int, [C.c_void_p, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
+    "ldp_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(JobOpts), C.POINTER(C.c_uint64)]),
+    "ldp_server_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "ldp_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "ldp_server_job": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "ldp_server_release": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ldp_server_info_get": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
+    "ldp_server_destroy": (None, [C.c_void_p]),
     "ldp_integrate_fp64_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(JobOpts), C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),
 }

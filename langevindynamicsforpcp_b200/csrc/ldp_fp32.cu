@@ -750,6 +750,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
             if (__builtin_expect(!(xp > lo && xp < hi) || fw <= thi || left == 0, 0)) {
                 sm.xp[t] = xp;
                 sm.rv[t] = rv;
+                sm.F[t] = F;
                 sm.left[t] = left;
                 sm.lo[t] = lo;
                 sm.hi[t] = hi;

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -31,7 +32,14 @@ struct Fp32Queue {
     uint64_t pair_budget = 1 << 15;
     int64_t nranges = 0;
     unsigned long long tail = 0;
-    int64_t* h_stage = nullptr;   // pinned staging for range/tail uploads
+    unsigned long long* rem = nullptr;   // [kFp32MaxJobs] trajectories not yet retired, by job slot
+    // Pinned staging for job uploads: a ring of 4 KiB blocks, each reused
+    // only after the copies that read it have run (its event), so that
+    // registering a job never waits for the launches in flight.
+    static constexpr int kStageSlots = 64;
+    int64_t* h_stage = nullptr;
+    cudaEvent_t stage_ev[kStageSlots] = {};
+    int stage_next = 0, stage_last = 0;
     std::vector<ldp_job*> table;  // job table slot -> job
     std::vector<int> free_slots;
 };
@@ -41,6 +49,16 @@ struct Fp32Runtime {
 };
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Next pinned staging block of the queue, once the copies that read it last
+// have run; the caller records stage_ev[stage_last] after its copies.
+static int64_t* stage(Fp32Queue& Q) {
+    const int si = Q.stage_next;
+    Q.stage_next = (Q.stage_next + 1) % Fp32Queue::kStageSlots;
+    cudaEventSynchronize(Q.stage_ev[si]);
+    Q.stage_last = si;
+    return Q.h_stage + (size_t)si * (4096 / sizeof(int64_t));
+}
 
 static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     if (Q.ready) return 0;
@@ -55,7 +73,8 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     const int64_t nslots = (int64_t)Q.grid * Q.block;
     // queue + job table
     size_t qb = al256(sizeof(int64_t) * kFp32MaxRanges) * 2 + al256(sizeof(int32_t) * kFp32MaxRanges) +
-                al256(sizeof(unsigned long long) * 2) + al256(sizeof(int32_t)) + al256(sizeof(JobF) * kFp32MaxJobs);
+                al256(sizeof(unsigned long long) * 2) + al256(sizeof(int32_t)) + al256(sizeof(JobF) * kFp32MaxJobs) +
+                al256(sizeof(unsigned long long) * kFp32MaxJobs);
     cudaError_t e = cudaMalloc(&Q.qmem, qb);
     if (e != cudaSuccess) return (int)e;
     cudaMemset(Q.qmem, 0, qb);
@@ -68,7 +87,8 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     Q.q.tail = Q.q.head + 1;
     o += al256(sizeof(unsigned long long) * 2);
     Q.q.nranges = (int32_t*)(a + o); o += al256(sizeof(int32_t));
-    Q.q.jobs = (JobF*)(a + o);
+    Q.q.jobs = (JobF*)(a + o); o += al256(sizeof(JobF) * kFp32MaxJobs);
+    Q.rem = (unsigned long long*)(a + o);
     // slots
     const int R = ring_slots;
     size_t sb = al256(sizeof(int32_t) * nslots) * 6 + al256(sizeof(int64_t) * nslots) * 6 +
@@ -101,8 +121,12 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     // every slot starts empty
     std::vector<int32_t> neg((size_t)nslots, -1);
     cudaMemcpy(S.job, neg.data(), sizeof(int32_t) * nslots, cudaMemcpyHostToDevice);
-    e = cudaMallocHost((void**)&Q.h_stage, 4096);
+    e = cudaMallocHost((void**)&Q.h_stage, 4096 * Fp32Queue::kStageSlots);
     if (e != cudaSuccess) return (int)e;
+    for (int i = 0; i < Fp32Queue::kStageSlots; ++i) {
+        e = cudaEventCreateWithFlags(&Q.stage_ev[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) return (int)e;
+    }
     Q.table.assign(kFp32MaxJobs, nullptr);
     Q.free_slots.clear();
     for (int i = kFp32MaxJobs - 1; i >= 0; --i) Q.free_slots.push_back(i);
@@ -191,52 +215,99 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
     J->init_idx0 = b; J->init_idx1 = b + n; J->idx2_0 = b + 2 * n; J->idx2_1 = b + 3 * n; J->tpt2_well = b + 4 * n;
     J->cg_well = b + 5 * n;
     J->cg_last = S.cg_well;   // int64 [ncg][n]
-    J->remaining = (unsigned long long*)job->d_aux;
+    J->remaining = nullptr;   // the queue's counter of the job's slot, set at registration
 }
 
 int fp32_type_of(const ldp_job* job) { return (job->k.dbl ? 2 : 0) + (job->k.over ? 1 : 0); }
+
+// One persistent launch of a queue with a given pair budget (serving).
+int fp32_launch_type(ldp_ctx* ctx, int type, uint32_t pair_budget, cudaStream_t st) {
+    Fp32Queue& Q = ctx->fp32->q[type];
+    if (!Q.ready) return 0;
+    return launch_fp32_persistent(type >= 2, (type & 1) != 0, Q.q, Q.s, pair_budget, Q.grid, Q.block, st);
+}
+
+// Asynchronous copy of a queue's per-slot remaining counters and of its
+// claimed-items count (serving).
+int fp32_copy_remaining(ldp_ctx* ctx, int type, unsigned long long* host, unsigned long long* head,
+                        cudaStream_t st) {
+    Fp32Queue& Q = ctx->fp32->q[type];
+    if (!Q.ready) return 0;
+    cudaError_t e = cudaMemcpyAsync(host, Q.rem, sizeof(unsigned long long) * kFp32MaxJobs,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(head, Q.q.head, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    return (int)e;
+}
+
+// Slots of a queue's persistent grid and items published so far (serving).
+int64_t fp32_nslots(ldp_ctx* ctx, int type) {
+    const Fp32Queue& Q = ctx->fp32->q[type];
+    return Q.ready ? Q.s.nslots : 0;
+}
+unsigned long long fp32_published(ldp_ctx* ctx, int type) {
+    const Fp32Queue& Q = ctx->fp32->q[type];
+    return Q.ready ? Q.tail : 0;
+}
 
 static Fp32Runtime* runtime(ldp_ctx* ctx) {
     if (!ctx->fp32) ctx->fp32 = new Fp32Runtime();
     return ctx->fp32;
 }
 
-// Registers the job and publishes its trajectories.
-int fp32_register(ldp_job* job) {
+// Registers the job (job table entry, remaining counter) and, unless
+// publish is false, publishes all its trajectories as one item range.
+int fp32_register(ldp_job* job, cudaStream_t stream, bool publish) {
     ldp_ctx* ctx = job->ctx;
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = stream ? stream : ctx->stream;
     Fp32Runtime* rt = runtime(ctx);
     const int type = fp32_type_of(job);
     Fp32Queue& Q = rt->q[type];
     int e = queue_init(ctx, Q, type, ctx->fp32_ring_slots ? ctx->fp32_ring_slots : 64);
     if (e) return e;
-    if (Q.free_slots.empty() || Q.nranges >= kFp32MaxRanges) return (int)cudaErrorMemoryAllocation;
+    if (Q.free_slots.empty()) return (int)cudaErrorMemoryAllocation;
     const int slot = Q.free_slots.back();
     Q.free_slots.pop_back();
     Q.table[slot] = job;
     job->fp32_type = type;
     job->fp32_slot = slot;
+    job->fp32_published = 0;
     JobF J;
     fill_jobf(job, &J);
-    // The JobF and the range are staged in pinned memory so the copies stay
-    // asynchronous; the stage is reused only after the stream has drained it.
-    cudaStreamSynchronize(st);
+    J.remaining = &Q.rem[slot];
+    int64_t* h = stage(Q);
     static_assert(sizeof(JobF) <= 4096 - 64, "JobF must fit the staging buffer");
-    std::memcpy(Q.h_stage + 8, &J, sizeof(J));
-    unsigned long long remaining = (unsigned long long)job->ntraj;
-    Q.h_stage[0] = (int64_t)remaining;
-    cudaMemcpyAsync(J.remaining, &Q.h_stage[0], sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(&Q.q.jobs[slot], Q.h_stage + 8, sizeof(J), cudaMemcpyHostToDevice, st);
+    std::memcpy(h + 8, &J, sizeof(J));
+    h[0] = (int64_t)job->ntraj;
+    cudaMemcpyAsync(J.remaining, &h[0], sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&Q.q.jobs[slot], h + 8, sizeof(J), cudaMemcpyHostToDevice, st);
+    cudaEventRecord(Q.stage_ev[Q.stage_last], st);
+    ++job->launches;
+    if (publish) return fp32_publish_range(job, job->ntraj, st);
+    return (int)cudaGetLastError();
+}
+
+// Publishes the job's next `count` trajectories (after those published
+// already) as one item range.
+int fp32_publish_range(ldp_job* job, int64_t count, cudaStream_t stream) {
+    ldp_ctx* ctx = job->ctx;
+    cudaStream_t st = stream ? stream : ctx->stream;
+    Fp32Queue& Q = ctx->fp32->q[job->fp32_type];
+    count = std::min<int64_t>(count, job->ntraj - job->fp32_published);
+    if (count <= 0) return 0;
+    if (Q.nranges >= kFp32MaxRanges) return (int)cudaErrorMemoryAllocation;
+    int64_t* h = stage(Q);
     const int64_t r = Q.nranges;
-    Q.tail += (unsigned long long)job->ntraj;
-    Q.h_stage[1] = (int64_t)Q.tail;       // range_end
-    Q.h_stage[2] = 0;                      // range_first
-    Q.h_stage[3] = slot;                   // range_job (low 32 bits)
-    cudaMemcpyAsync(&Q.q.range_end[r], &Q.h_stage[1], sizeof(int64_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(&Q.q.range_first[r], &Q.h_stage[2], sizeof(int64_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(&Q.q.range_job[r], &Q.h_stage[3], sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    Q.tail += (unsigned long long)count;
+    h[1] = (int64_t)Q.tail;               // range_end
+    h[2] = job->fp32_published;           // range_first
+    h[3] = job->fp32_slot;                // range_job (low 32 bits)
+    cudaMemcpyAsync(&Q.q.range_end[r], &h[1], sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&Q.q.range_first[r], &h[2], sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&Q.q.range_job[r], &h[3], sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    cudaEventRecord(Q.stage_ev[Q.stage_last], st);
     Q.nranges = r + 1;
-    e = launch_fp32_publish(Q.q, Q.tail, (int32_t)Q.nranges, st);
+    job->fp32_published += count;
+    const int e = launch_fp32_publish(Q.q, Q.tail, (int32_t)Q.nranges, st);
     if (e) return e;
     ++job->launches;
     return (int)cudaGetLastError();
@@ -269,8 +340,19 @@ int fp32_estimate_launches(const ldp_job* job) {
     return std::min(n, 4096);
 }
 
+// Persistent launches that drain the type's queue for certain: a work-
+// conserving list schedule of independent trajectories on m slots ends
+// within total/m + longest (Graham's bound), in pairs of the launch budget.
+int fp32_launch_bound(ldp_ctx* ctx, int type, double total_pairs, double max_pairs) {
+    const Fp32Queue& Q = ctx->fp32->q[type];
+    const double pb = (double)std::min<uint64_t>(Q.pair_budget, 0xffffffffull);
+    const double n = std::ceil(total_pairs / ((double)Q.s.nslots * pb)) + std::ceil(max_pairs / pb) + 1.0;
+    return (int)std::min(n, 1.0e6);
+}
+
 int fp32_remaining(ldp_job* job, unsigned long long* rem) {
-    return (int)cudaMemcpy(rem, job->d_aux, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    const Fp32Queue& Q = job->ctx->fp32->q[job->fp32_type];
+    return (int)cudaMemcpy(rem, &Q.rem[job->fp32_slot], sizeof(unsigned long long), cudaMemcpyDeviceToHost);
 }
 
 __global__ void ssum_to_time_kernel(const int64_t* ssum, double* sums, double dt, int64_t n) {
@@ -280,8 +362,8 @@ __global__ void ssum_to_time_kernel(const int64_t* ssum, double* sums, double dt
 
 // Post-processing after all trajectories retired: event-duration sums in
 // time units, then the MSD of the saved frames.
-int fp32_finalize(ldp_job* job) {
-    cudaStream_t st = job->ctx->stream;
+int fp32_finalize(ldp_job* job, cudaStream_t stream) {
+    cudaStream_t st = stream ? stream : job->ctx->stream;
     const int64_t n = (int64_t)LDP_NSUM * job->ntraj;
     ssum_to_time_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(job->d_ssum, job->st.sums, job->k.dt, n);
     int e = (int)cudaGetLastError();
@@ -310,6 +392,8 @@ void fp32_destroy_runtime(ldp_ctx* ctx) {
         if (Q.qmem) cudaFree(Q.qmem);
         if (Q.smem) cudaFree(Q.smem);
         if (Q.h_stage) cudaFreeHost(Q.h_stage);
+        for (auto& ev : Q.stage_ev)
+            if (ev) cudaEventDestroy(ev);
     }
     delete ctx->fp32;
     ctx->fp32 = nullptr;

@@ -51,8 +51,10 @@ struct ldp_job {
     int32_t* d_i32b = nullptr;   // FP32 batched: 32-bit statistics state
     int fp32_type = -1;          // FP32 batched: queue (dbl*2 + over) the job is in
     int fp32_slot = -1;          // FP32 batched: index in that queue's job table
+    int64_t fp32_published = 0;  // FP32 batched: trajectories published to the queue
     bool finalized = false;      // results post-processed after completion
-    int fp32_phase = 0;          // 0 idle, 1 integrating, 2 finalizing
+    int fp32_phase = 0;          // 0 idle, 1 integrating, 2 finalizing, 3 in a batch graph
+    cudaGraphExec_t gexec = nullptr;   // batch graph this job owns (first job of the batch)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool submitted = false;
     bool done = false;
@@ -65,12 +67,24 @@ struct ldp_job {
 void ldp_set_error(ldp_ctx* ctx, const char* fmt, ...);
 
 namespace ldp {
-int fp32_register(ldp_job* job);
+int fp32_register(ldp_job* job, cudaStream_t stream = nullptr, bool publish = true);
+int fp32_publish_range(ldp_job* job, int64_t count, cudaStream_t stream = nullptr);
 int fp32_pump(ldp_job* job, int nlaunch);
 int fp32_estimate_launches(const ldp_job* job);
+int fp32_launch_bound(ldp_ctx* ctx, int type, double total_pairs, double max_pairs);
 int fp32_remaining(ldp_job* job, unsigned long long* rem);
-int fp32_finalize(ldp_job* job);
+int fp32_type_of(const ldp_job* job);
+int fp32_launch_type(ldp_ctx* ctx, int type, uint32_t pair_budget, cudaStream_t st);
+int fp32_copy_remaining(ldp_ctx* ctx, int type, unsigned long long* host, unsigned long long* head,
+                        cudaStream_t st);
+int64_t fp32_nslots(ldp_ctx* ctx, int type);
+unsigned long long fp32_published(ldp_ctx* ctx, int type);
+int fp32_finalize(ldp_job* job, cudaStream_t stream = nullptr);
 void fp32_release(ldp_job* job);
 void fp32_destroy_runtime(ldp_ctx* ctx);
 }  // namespace ldp
 std::vector<int64_t> ldp_lag_grid(const ldp_params& p);
+// Job creation without the free-memory check, and the job's device arena
+// (size, or allocation): the serving loop admits jobs by footprint itself.
+ldp_status ldp_job_create_unchecked(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out);
+size_t ldp_job_arena(ldp_job* job, bool alloc);

@@ -343,7 +343,19 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     return off;
 }
 
+size_t ldp_job_arena(ldp_job* job, bool alloc) { return job_arena(job, alloc); }
+
+static ldp_status job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out, bool check_mem);
+
 extern "C" ldp_status ldp_job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out) {
+    return job_create(ctx, p, o, out, true);
+}
+
+ldp_status ldp_job_create_unchecked(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out) {
+    return job_create(ctx, p, o, out, false);
+}
+
+static ldp_status job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out, bool check_mem) {
     if (!ctx || !p || !out) return LDP_ERR_INVALID;
     *out = nullptr;
     ldp_job_opts opts;
@@ -390,7 +402,7 @@ extern "C" ldp_status ldp_job_create(ldp_ctx* ctx, const ldp_params* p, const ld
     cudaSetDevice(ctx->device);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    if (need + ((size_t)256 << 20) > free_b) {
+    if (check_mem && need + ((size_t)256 << 20) > free_b) {
         ldp_set_error(ctx, "job needs %.2f GB of device memory, %.2f GB free", need / 1e9, free_b / 1e9);
         delete job;
         return LDP_ERR_NOMEM;
@@ -499,6 +511,16 @@ static ldp_status fp32_advance(ldp_ctx* ctx, ldp_job* job, int* done) {
         job->fp32_phase = 2;
         return LDP_OK;
     }
+    if (job->fp32_phase == 3) {
+        // The batch graph ran every launch its bound allows and the
+        // post-processing after them; all trajectories must have retired.
+        unsigned long long rem = 0;
+        CUDA_OR_FAIL(ctx, (cudaError_t)fp32_remaining(job, &rem));
+        if (rem > 0) {
+            ldp_set_error(ctx, "batch graph ended with %llu trajectories not retired", rem);
+            return LDP_ERR_DEVICE;
+        }
+    }
     job->fp32_phase = 0;
     fp32_release(job);
     *done = 1;
@@ -553,6 +575,7 @@ extern "C" ldp_status ldp_job_info_get(const ldp_job* job, ldp_job_info* info) {
     info->precision = job->o.precision;
     info->mode = job->o.mode;
     info->done = job->done ? 1 : 0;
+    info->device_bytes = (int64_t)job_arena(const_cast<ldp_job*>(job), false);
     return LDP_OK;
 }
 
@@ -580,6 +603,7 @@ extern "C" void ldp_job_destroy(ldp_job* job) {
     cudaSetDevice(job->ctx->device);
     if (job->submitted && !job->done) ldp_wait(job->ctx, job);
     fp32_release(job);
+    if (job->gexec) cudaGraphExecDestroy(job->gexec);
     for (int i = 0; i < 4; ++i)
         if (job->ev[i]) cudaEventDestroy(job->ev[i]);
     if (job->arena) cudaFreeAsync(job->arena, job->ctx->stream);
@@ -718,6 +742,76 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[1], s));
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[2], s));
         job->fp32_phase = 1;
+    }
+    return LDP_OK;
+}
+
+// Registers every job, then runs all their persistent launches and their
+// post-processing as one CUDA graph: the launch count is an upper bound for
+// draining the queues, so no host round trip happens until the results.
+extern "C" ldp_status ldp_submit_batch_graph(ldp_ctx* ctx, ldp_job** jobs, int njobs) {
+    if (!ctx || !jobs || njobs < 1) return LDP_ERR_INVALID;
+    CUDA_OR_FAIL(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    for (int i = 0; i < njobs; ++i) {
+        ldp_job* job = jobs[i];
+        if (!job || job->submitted || job->ctx != ctx || job->o.precision != LDP_PREC_FP32_BATCHED) {
+            ldp_set_error(ctx, "job %d is null, submitted already, of another context or not FP32 batched", i);
+            return LDP_ERR_INVALID;
+        }
+    }
+    double total[4] = {0, 0, 0, 0}, longest[4] = {0, 0, 0, 0};
+    for (int i = 0; i < njobs; ++i) {
+        ldp_job* job = jobs[i];
+        if (!job->arena && job_arena(job, true) == 0) {
+            ldp_set_error(ctx, "cudaMalloc of %zu bytes failed", job_arena(job, false));
+            return LDP_ERR_NOMEM;
+        }
+        job->launches = 0;
+        int e = fp32_register(job);
+        if (e) {
+            ldp_set_error(ctx, "FP32 registration failed: %s", cudaGetErrorString((cudaError_t)e));
+            return LDP_ERR_DEVICE;
+        }
+        job->submitted = true;
+        const int t = job->fp32_type;
+        const double pairs = (double)((job->nsteps + 1) / 2);
+        total[t] += pairs * (double)job->ntraj;
+        longest[t] = std::max(longest[t], pairs);
+    }
+    CUDA_OR_FAIL(ctx, cudaEventRecord(jobs[0]->ev[0], s));
+    CUDA_OR_FAIL(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    int e = 0;
+    for (int t = 0; t < 4 && !e; ++t) {
+        if (total[t] <= 0.0) continue;
+        ldp_job* first = nullptr;
+        for (int i = 0; i < njobs; ++i)
+            if (jobs[i]->fp32_type == t) { first = jobs[i]; break; }
+        e = fp32_pump(first, fp32_launch_bound(ctx, t, total[t], longest[t]));
+    }
+    for (int i = 0; i < njobs && !e; ++i) e = fp32_finalize(jobs[i]);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+    if (e || ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        ldp_set_error(ctx, "batch graph capture failed: %s", cudaGetErrorString(e ? (cudaError_t)e : ec));
+        return LDP_ERR_DEVICE;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        ldp_set_error(ctx, "batch graph instantiation failed: %s", cudaGetErrorString(ei));
+        return LDP_ERR_DEVICE;
+    }
+    jobs[0]->gexec = exec;
+    CUDA_OR_FAIL(ctx, cudaGraphLaunch(exec, s));
+    for (int i = 0; i < njobs; ++i) {
+        ldp_job* job = jobs[i];
+        if (i) CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[0], s));
+        CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[1], s));
+        CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[2], s));
+        job->fp32_phase = 3;
     }
     return LDP_OK;
 }

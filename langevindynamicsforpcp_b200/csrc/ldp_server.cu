@@ -1,0 +1,411 @@
+// ldp_server.cu -- serving loop: continuous batching of FP32 batched jobs.
+//
+// Requests (.inp parameter sets with job options) are submitted at any time
+// and from any thread; each step of the loop
+//  1. admits queued jobs in arrival order while their device footprint fits
+//     the memory budget (a job larger than the whole budget is admitted
+//     alone), allocating their arena and registering them with the work
+//     queue of their model type;
+//  2. publishes admitted jobs' trajectories to the queue in chunks, keeping
+//     about one wave of slots' worth of unclaimed work queued and always
+//     publishing next for the job with the fewest unpublished trajectories
+//     (shortest remaining first): a small job that arrives while large ones
+//     run starts within one chunk, instead of after every earlier job;
+//  3. keeps up to `max_inflight` short persistent launches (pair budget
+//     `pair_budget`) in flight per model type with active jobs, each type on
+//     its own stream, so the types share the GPU and newly published work is
+//     reached within one launch;
+//  4. reads every queue's per-job "trajectories not yet retired" counters
+//     (and its claimed-items count) with one asynchronous copy, and for each
+//     job whose counter reached zero enqueues its post-processing (event
+//     sums, MSD) on a separate stream;
+//  5. marks jobs done when their post-processing has run.
+// A context that runs a server should not also run FP32 batched jobs
+// through ldp_submit: the server's streams order the queues' work.
+// Job state (RNG counters, partial statistics) stays in HBM from admission
+// to release; results are identical alone and in any mix, since every draw
+// is keyed by (seed, job id, trajectory, step).
+//
+// The reference runs one .inp per MPI process (src/mpiKernel.cpp); the
+// serving loop has no counterpart there.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "ldp_fp32.h"
+#include "ldp_internal.h"
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Entry {
+    uint64_t ticket = 0;
+    ldp_job* job = nullptr;
+    size_t bytes = 0;
+    int state = LDP_SRV_QUEUED;
+    int type = -1;
+    uint64_t gen_admit = 0;          // remaining-counter copies issued before admission
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    cudaEvent_t fin = nullptr;       // post-processing done
+};
+
+}  // namespace
+
+struct ldp_server {
+    ldp_ctx* ctx = nullptr;
+    size_t budget = 0, in_use = 0;
+    uint32_t pair_budget = 0;
+    int max_inflight = 2;
+    cudaStream_t side = nullptr;         // post-processing
+    cudaStream_t qs[4] = {};             // one per model type: publication, launches, counter copies
+    unsigned long long head_seen[4] = {};
+    std::mutex mu;                       // guards pending and all
+    std::deque<Entry*> pending;
+    std::vector<Entry*> running;         // integrating
+    std::vector<Entry*> finishing;       // post-processing enqueued
+    std::unordered_map<uint64_t, Entry*> all;
+    uint64_t next_ticket = 1;
+    unsigned long long* h_rem[4] = {};   // pinned copies of the queues' counters
+    cudaEvent_t rem_ev[4] = {};
+    bool rem_pending[4] = {};
+    uint64_t rem_gen[4] = {};            // copies issued per type
+    std::deque<cudaEvent_t> inflight[4];
+    std::vector<cudaEvent_t> pool;       // idle events
+    int64_t launches = 0;
+
+    cudaEvent_t get_event() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        return e;
+    }
+};
+
+static ldp_status fail(ldp_server* s, const char* what, cudaError_t e) {
+    ldp_set_error(s->ctx, "%s: %s", what, cudaGetErrorString(e));
+    return LDP_ERR_DEVICE;
+}
+
+extern "C" void ldp_server_opts_default(ldp_server_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->hbm_budget = 0;        // 80% of the free device memory at creation
+    o->pair_budget = 2048;    // step pairs per slot per launch
+    o->max_inflight = 2;
+}
+
+extern "C" ldp_status ldp_server_create(ldp_ctx* ctx, const ldp_server_opts* o, ldp_server** out) {
+    if (!ctx || !out) return LDP_ERR_INVALID;
+    ldp_server_opts opts;
+    if (o) opts = *o; else ldp_server_opts_default(&opts);
+    if (opts.max_inflight < 1 || opts.max_inflight > 16) {
+        ldp_set_error(ctx, "max_inflight must be 1..16 (got %d)", opts.max_inflight);
+        return LDP_ERR_INVALID;
+    }
+    cudaSetDevice(ctx->device);
+    ldp_server* s = new ldp_server();
+    s->ctx = ctx;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    s->budget = opts.hbm_budget ? (size_t)opts.hbm_budget : (size_t)(0.8 * (double)free_b);
+    s->pair_budget = opts.pair_budget ? (uint32_t)opts.pair_budget : 2048u;
+    s->max_inflight = opts.max_inflight;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    for (int t = 0; t < 4 && e == cudaSuccess; ++t) {
+        // the queue's counters, then its claimed-items count
+        e = cudaMallocHost((void**)&s->h_rem[t], sizeof(unsigned long long) * (ldp::kFp32MaxJobs + 1));
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->rem_ev[t], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->qs[t], cudaStreamNonBlocking);
+    }
+    if (e != cudaSuccess) {
+        ldp_server_destroy(s);
+        ldp_set_error(ctx, "server set-up failed: %s", cudaGetErrorString(e));
+        return LDP_ERR_DEVICE;
+    }
+    *out = s;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_submit(ldp_server* s, const ldp_params* p, const ldp_job_opts* o,
+                                        uint64_t* ticket) {
+    if (!s || !p || !ticket) return LDP_ERR_INVALID;
+    ldp_job_opts opts;
+    if (o) opts = *o; else ldp_job_opts_default(&opts);
+    if (opts.precision != LDP_PREC_FP32_BATCHED) {
+        ldp_set_error(s->ctx, "the serving loop runs FP32 batched jobs");
+        return LDP_ERR_UNSUPPORTED;
+    }
+    ldp_job* job = nullptr;
+    ldp_status st = ldp_job_create_unchecked(s->ctx, p, &opts, &job);
+    if (st != LDP_OK) return st;
+    Entry* en = new Entry();
+    en->job = job;
+    en->bytes = ldp_job_arena(job, false);
+    en->type = (job->k.dbl ? 2 : 0) + (job->k.over ? 1 : 0);
+    en->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(s->mu);
+    en->ticket = s->next_ticket++;
+    s->pending.push_back(en);
+    s->all[en->ticket] = en;
+    *ticket = en->ticket;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
+    if (!s) return LDP_ERR_INVALID;
+    ldp_ctx* ctx = s->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    int done = 0;
+
+    // 1. admission, in arrival order, by footprint
+    for (;;) {
+        Entry* en = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->pending.empty()) break;
+            en = s->pending.front();
+            const bool idle = s->running.empty() && s->finishing.empty();
+            if (!idle && s->in_use + en->bytes > s->budget) break;
+            s->pending.pop_front();
+        }
+        ldp_job* job = en->job;
+        if (ldp_job_arena(job, true) == 0) {
+            const bool idle = s->running.empty() && s->finishing.empty();
+            if (idle) {
+                en->state = LDP_SRV_FAILED;
+                en->t_done = now_s();
+                ldp_set_error(ctx, "job %llu: device allocation of %zu bytes failed",
+                              (unsigned long long)en->ticket, en->bytes);
+                continue;
+            }
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->pending.push_front(en);
+            break;
+        }
+        job->launches = 0;
+        // the arena was allocated on the context's stream
+        cudaEvent_t ready = s->get_event();
+        cudaEventRecord(ready, st);
+        cudaStreamWaitEvent(s->qs[en->type], ready, 0);
+        s->pool.push_back(ready);
+        const int e = ldp::fp32_register(job, s->qs[en->type], false);
+        if (e) return fail(s, "job registration", (cudaError_t)e);
+        job->submitted = true;
+        job->fp32_phase = 1;
+        en->state = LDP_SRV_RUNNING;
+        en->gen_admit = s->rem_gen[en->type];
+        en->t_admit = now_s();
+        s->in_use += en->bytes;
+        s->running.push_back(en);
+    }
+
+    // 2. publication: about one wave of unclaimed work per type, shortest
+    //    remaining job first
+    bool active[4] = {false, false, false, false};
+    for (Entry* en : s->running) active[en->type] = true;
+    for (int t = 0; t < 4; ++t) {
+        if (!active[t]) continue;
+        const int64_t wave = ldp::fp32_nslots(ctx, t);
+        const unsigned long long pub = ldp::fp32_published(ctx, t);
+        int64_t backlog = (int64_t)(pub - std::min(pub, s->head_seen[t]));
+        while (backlog < wave) {
+            Entry* best = nullptr;
+            int64_t best_left = 0;
+            for (Entry* en : s->running) {
+                if (en->type != t) continue;
+                const int64_t left = en->job->ntraj - en->job->fp32_published;
+                if (left > 0 && (!best || left < best_left)) { best = en; best_left = left; }
+            }
+            if (!best) break;
+            const int64_t chunk = std::min<int64_t>(best_left, std::max<int64_t>(wave - backlog, 1024));
+            const int e = ldp::fp32_publish_range(best->job, chunk, s->qs[t]);
+            if (e) return fail(s, "publication", (cudaError_t)e);
+            backlog += chunk;
+        }
+    }
+
+    // 3. persistent launches of every type with work
+    for (int t = 0; t < 4; ++t) {
+        auto& q = s->inflight[t];
+        while (!q.empty() && cudaEventQuery(q.front()) == cudaSuccess) {
+            s->pool.push_back(q.front());
+            q.pop_front();
+        }
+        if (!active[t]) continue;
+        while ((int)q.size() < s->max_inflight) {
+            const int e = ldp::fp32_launch_type(ctx, t, s->pair_budget, s->qs[t]);
+            if (e) return fail(s, "persistent launch", (cudaError_t)e);
+            ++s->launches;
+            cudaEvent_t ev = s->get_event();
+            cudaEventRecord(ev, s->qs[t]);
+            q.push_back(ev);
+        }
+    }
+
+    // 4. completion: one counter copy per type, read when it has landed
+    for (int t = 0; t < 4; ++t) {
+        if (s->rem_pending[t]) {
+            const cudaError_t q = cudaEventQuery(s->rem_ev[t]);
+            if (q == cudaErrorNotReady) continue;
+            if (q != cudaSuccess) return fail(s, "counter copy", q);
+            s->rem_pending[t] = false;
+            s->head_seen[t] = s->h_rem[t][ldp::kFp32MaxJobs];
+            const uint64_t gen = s->rem_gen[t];
+            for (size_t i = 0; i < s->running.size();) {
+                Entry* en = s->running[i];
+                // a copy issued before the job was registered holds the
+                // counter of the slot's previous job
+                if (en->type != t || en->gen_admit >= gen || s->h_rem[t][en->job->fp32_slot] != 0) {
+                    ++i;
+                    continue;
+                }
+                cudaStreamWaitEvent(s->side, s->rem_ev[t], 0);
+                const int e = ldp::fp32_finalize(en->job, s->side);
+                if (e) return fail(s, "post-processing", (cudaError_t)e);
+                en->fin = s->get_event();
+                cudaEventRecord(en->fin, s->side);
+                en->state = LDP_SRV_FINISHING;
+                en->job->fp32_phase = 2;
+                s->finishing.push_back(en);
+                s->running[i] = s->running.back();
+                s->running.pop_back();
+            }
+        }
+        if (!s->rem_pending[t]) {
+            bool any = false;
+            for (Entry* en : s->running) any = any || en->type == t;
+            if (!any) continue;
+            const int e = ldp::fp32_copy_remaining(ctx, t, s->h_rem[t], s->h_rem[t] + ldp::kFp32MaxJobs, s->qs[t]);
+            if (e) return fail(s, "counter copy", (cudaError_t)e);
+            cudaEventRecord(s->rem_ev[t], s->qs[t]);
+            s->rem_pending[t] = true;
+            ++s->rem_gen[t];
+        }
+    }
+
+    // 5. jobs whose post-processing ran
+    for (size_t i = 0; i < s->finishing.size();) {
+        Entry* en = s->finishing[i];
+        const cudaError_t q = cudaEventQuery(en->fin);
+        if (q == cudaErrorNotReady) { ++i; continue; }
+        if (q != cudaSuccess) return fail(s, "post-processing", q);
+        s->pool.push_back(en->fin);
+        en->fin = nullptr;
+        ldp_job* job = en->job;
+        job->fp32_phase = 0;
+        ldp::fp32_release(job);
+        job->done = true;
+        en->state = LDP_SRV_DONE;
+        en->t_done = now_s();
+        ++done;
+        s->finishing[i] = s->finishing.back();
+        s->finishing.pop_back();
+    }
+    if (ndone) *ndone = done;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_poll(ldp_server* s, uint64_t ticket, int* state, double* latency_s) {
+    if (!s || !state) return LDP_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return LDP_ERR_INVALID;
+    const Entry* en = it->second;
+    *state = en->state;
+    if (latency_s) *latency_s = (en->state == LDP_SRV_DONE || en->state == LDP_SRV_FAILED) ? en->t_done - en->t_submit
+                                                                                          : 0.0;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_job(ldp_server* s, uint64_t ticket, ldp_job** job) {
+    if (!s || !job) return LDP_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end() || it->second->state != LDP_SRV_DONE) return LDP_ERR_NOT_READY;
+    *job = it->second->job;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_release(ldp_server* s, uint64_t ticket) {
+    if (!s) return LDP_ERR_INVALID;
+    Entry* en = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->all.find(ticket);
+        if (it == s->all.end()) return LDP_ERR_INVALID;
+        en = it->second;
+        if (en->state != LDP_SRV_DONE && en->state != LDP_SRV_FAILED) return LDP_ERR_NOT_READY;
+        s->all.erase(it);
+    }
+    if (en->state == LDP_SRV_DONE) s->in_use -= en->bytes;
+    ldp_job_destroy(en->job);
+    delete en;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_info_get(ldp_server* s, ldp_server_info* info) {
+    if (!s || !info) return LDP_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::memset(info, 0, sizeof(*info));
+    info->queued = (int64_t)s->pending.size();
+    info->running = (int64_t)s->running.size();
+    info->finishing = (int64_t)s->finishing.size();
+    int64_t d = 0;
+    for (auto& kv : s->all) d += kv.second->state == LDP_SRV_DONE;
+    info->done = d;
+    info->hbm_in_use = (int64_t)s->in_use;
+    info->hbm_budget = (int64_t)s->budget;
+    info->launches = s->launches;
+    return LDP_OK;
+}
+
+extern "C" void ldp_server_destroy(ldp_server* s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    if (s->side) cudaStreamSynchronize(s->side);
+    for (int t = 0; t < 4; ++t)
+        if (s->qs[t]) cudaStreamSynchronize(s->qs[t]);
+    {
+        // Jobs never admitted are dropped; jobs still integrating hold queue
+        // slots until their trajectories retired, so the loop runs on until
+        // nothing is active.
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->pending.clear();
+    }
+    for (int guard = 0; guard < 100000 && (!s->running.empty() || !s->finishing.empty()); ++guard) {
+        if (ldp_server_step(s, nullptr) != LDP_OK) break;
+        cudaStreamSynchronize(s->side);
+        for (int t = 0; t < 4; ++t) cudaStreamSynchronize(s->qs[t]);
+    }
+    for (auto& kv : s->all) {
+        if (kv.second->fin) cudaEventDestroy(kv.second->fin);
+        ldp_job_destroy(kv.second->job);
+        delete kv.second;
+    }
+    for (int t = 0; t < 4; ++t) {
+        for (cudaEvent_t e : s->inflight[t]) cudaEventDestroy(e);
+        if (s->rem_ev[t]) cudaEventDestroy(s->rem_ev[t]);
+        if (s->h_rem[t]) cudaFreeHost(s->h_rem[t]);
+    }
+    for (cudaEvent_t e : s->pool) cudaEventDestroy(e);
+    if (s->side) cudaStreamDestroy(s->side);
+    for (int t = 0; t < 4; ++t)
+        if (s->qs[t]) cudaStreamDestroy(s->qs[t]);
+    delete s;
+}

@@ -1,0 +1,234 @@
+"""Serving: a request loop over the library's serving loop (ldp_server_*).
+
+Jobs (.inp parameter sets) arrive over time; the C++ serving loop admits
+them by device-memory footprint, runs them in the shared persistent launches
+of their model type while other jobs are in flight (continuous batching) and
+finishes each one as soon as its trajectories have all retired.  This module
+adds the request side: a Poisson arrival stream, per-job latency, and the
+"serving" workload -- jobs of random type (single or double barrier, under-
+or overdamped), parameters from the precision / batching / scan ranges,
+trajectory counts 2^U[10, 18], seed 1234.  The reference runs one .inp per
+MPI process; serving has no counterpart there.
+
+    python -m langevindynamicsforpcp_b200.serve [--jobs N] [--loads 0.5 0.8]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from . import (Context, Job, MODEL_DOUBLE, MODEL_SINGLE, MODE_FIXED_STEPS, PREC_FP32_BATCHED, _check,
+               params_from_inp_text)
+from . import _lib as L
+
+COMMON = """\
+OUTPUTBASE serve
+OVERDAMPED {over}
+V0 1.0
+GAMMA {gamma!r}
+KB 1.0
+TEMPERATURE 1.0
+MASS 1.0
+RANDOMIZEV true
+PERIODICLENGTH 5.8
+X0 -2.9
+TIMESTEP 1.0e-5
+NUMBEROFSTEPS {steps}
+NUMBEROFPREVIOUSSTEPS 0
+NUMBEROFRUNS 1
+FREQSAVE {freq}
+FREQSTAT 1
+DISTRIBUTIONV0 false
+DISTRIBUTIONS0 true
+TAU {tau!r}
+INITIALSTATE 0
+RANDOMIZESTATES true
+UNIFORMINITALSTATES false
+EQ true 1.0
+WAITINGTIME false
+FPT true
+TPT true
+FPTCG true 2
+FPTCG true 10
+READRESTART false
+WRITERESTART false
+INPUTRESTART none
+OUTPUTRESTART none
+WRITEX false
+NUMBEROFLOGSAMPLES 40
+RANDOMSEED {seed}
+PRINTTIMER false
+"""
+SINGLE = "BARRIERHEIGHTS {high!r} {low!r}\nBARRIERHALFWIDTH 0.65\n"
+DOUBLE = ("BARRIERHEIGHTS0 {mid!r} {low!r}\nBARRIERHEIGHTS1 {high!r} {low!r}\nBARRIERHALFWIDTH0 0.70\n"
+          "BARRIERHALFWIDTH1 0.65\nBARRIERPOSITION0 -1.42\nBARRIERPOSITION1 -0.56\n")
+
+
+class Server:
+    """The library's serving loop (ldp_server_create ... ldp_server_destroy)."""
+
+    def __init__(self, ctx: Context, hbm_budget: int = 0, pair_budget: int = 2048, max_inflight: int = 2):
+        self.ctx = ctx
+        o = L.ServerOpts()
+        L.lib().ldp_server_opts_default(C.byref(o))
+        o.hbm_budget, o.pair_budget, o.max_inflight = hbm_budget, pair_budget, max_inflight
+        h = C.c_void_p()
+        _check(L.lib().ldp_server_create(ctx.handle, C.byref(o), C.byref(h)), ctx)
+        self.handle = h
+
+    def submit(self, params, lanes: int, job_id: int = 0) -> int:
+        o = L.JobOpts()
+        L.lib().ldp_job_opts_default(C.byref(o))
+        o.lanes, o.ranks, o.precision, o.mode, o.job_id = lanes, 1, PREC_FP32_BATCHED, MODE_FIXED_STEPS, job_id
+        t = C.c_uint64()
+        _check(L.lib().ldp_server_submit(self.handle, C.byref(params), C.byref(o), C.byref(t)), self.ctx)
+        return t.value
+
+    def step(self) -> int:
+        n = C.c_int(0)
+        _check(L.lib().ldp_server_step(self.handle, C.byref(n)), self.ctx)
+        return n.value
+
+    def poll(self, ticket: int):
+        st, lat = C.c_int(0), C.c_double(0)
+        _check(L.lib().ldp_server_poll(self.handle, ticket, C.byref(st), C.byref(lat)), self.ctx)
+        return st.value, lat.value
+
+    def job(self, ticket: int) -> Job:
+        h = C.c_void_p()
+        _check(L.lib().ldp_server_job(self.handle, ticket, C.byref(h)), self.ctx)
+        return Job.borrowed(self.ctx, h)
+
+    def release(self, ticket: int) -> None:
+        _check(L.lib().ldp_server_release(self.handle, ticket), self.ctx)
+
+    def info(self) -> dict:
+        i = L.ServerInfo()
+        _check(L.lib().ldp_server_info_get(self.handle, C.byref(i)), self.ctx)
+        return {k: getattr(i, k) for k, _ in L.ServerInfo._fields_}
+
+    def close(self):
+        if self.handle:
+            L.lib().ldp_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def serving_workload(n: int, seed: int = 1234, exp_lo: float = 10, exp_hi: float = 18, steps: int = 24000,
+                     freq: int = 20):
+    """n jobs: (params, ntraj, label).  Type uniform over {single, double} x
+    {over-, underdamped}; H_low in {2, 3, 4, 5} (single: high 3.6 H; double:
+    barrier 0 high 1.7 H, barrier 1 high 3.6 H), flip rate k logU[1e-2, 1e2]
+    (TAU = 1/k), friction logU[0.1, 10]; CuIDB single/double geometry."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        dbl = bool(rng.integers(2))
+        over = bool(rng.integers(2))
+        h = float(rng.choice([2.0, 3.0, 4.0, 5.0]))
+        k = float(10 ** rng.uniform(-2, 2))
+        g = float(10 ** rng.uniform(-1, 1))
+        ntraj = int(2 ** rng.uniform(exp_lo, exp_hi))
+        text = COMMON.format(over="true" if over else "false", gamma=g, steps=steps, freq=freq, tau=1.0 / k,
+                             seed=seed)
+        text += (DOUBLE.format(mid=1.7 * h, high=3.6 * h, low=h) if dbl else SINGLE.format(high=3.6 * h, low=h))
+        p = params_from_inp_text(text, MODEL_DOUBLE if dbl else MODEL_SINGLE)
+        out.append((p, ntraj, {"double": dbl, "overdamped": over, "H": h, "k": k, "gamma": g, "ntraj": ntraj}))
+    return out
+
+
+def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 900.0):
+    """Submits work[i] at time arrivals[i] (seconds from now), drives the
+    loop until every job is done; returns per-job latency (submission to
+    done, seconds).  on_done(i, job) is called before each job is released."""
+    n = len(work)
+    lat = np.full(n, np.nan)
+    tickets = {}
+    nxt = 0
+    t0 = time.perf_counter()
+    while nxt < n or tickets:
+        now = time.perf_counter() - t0
+        if now > timeout_s:
+            raise TimeoutError(f"serving stream not finished after {timeout_s} s")
+        while nxt < n and arrivals[nxt] <= now:
+            p, ntraj, _ = work[nxt]
+            tickets[server.submit(p, ntraj, job_id=nxt)] = nxt
+            nxt += 1
+        if server.step() or True:
+            for t in list(tickets):
+                st, l = server.poll(t)
+                if st == L.SRV_DONE or st == L.SRV_FAILED:
+                    i = tickets.pop(t)
+                    if st == L.SRV_FAILED:
+                        raise RuntimeError(f"job {i} failed: {server.ctx.last_error()}")
+                    lat[i] = l
+                    if on_done:
+                        on_done(i, server.job(t))
+                    server.release(t)
+        if not tickets and nxt < n:
+            time.sleep(max(0.0, min(arrivals[nxt] - (time.perf_counter() - t0), 0.01)))
+    return lat
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--jobs", type=int, default=10000)
+    ap.add_argument("--exp-lo", type=float, default=10)
+    ap.add_argument("--exp-hi", type=float, default=18)
+    ap.add_argument("--steps", type=int, default=24000)
+    ap.add_argument("--loads", type=float, nargs="+", default=[0.5, 0.8])
+    ap.add_argument("--isolated-sample", type=int, default=24)
+    a = ap.parse_args(argv)
+    work = serving_workload(a.jobs, exp_lo=a.exp_lo, exp_hi=a.exp_hi, steps=a.steps)
+    psteps = float(sum(n for _, n, _ in work)) * a.steps
+    out = {"workload": f"serving: {a.jobs} jobs, types single/double x over/underdamped, "
+                       f"2^U[{a.exp_lo:g},{a.exp_hi:g}] trajectories, {a.steps} steps", "loads": {}}
+    with Context(0) as ctx, Server(ctx) as srv:
+        # capacity: every job submitted at once
+        t = time.perf_counter()
+        run_stream(srv, work, np.zeros(len(work)))
+        makespan = time.perf_counter() - t
+        cap = len(work) / makespan
+        out["capacity"] = {"jobs_per_s": cap, "particle_steps_per_s": psteps / makespan, "makespan_s": makespan}
+        # isolated solve times of a sample spanning the sizes, per type
+        rng = np.random.default_rng(7)
+        sample = rng.choice(len(work), size=min(a.isolated_sample, len(work)), replace=False)
+        iso = {}
+        for i in sample:
+            l = run_stream(srv, [work[i]], [0.0])
+            iso[int(i)] = float(l[0])
+        xs = np.array([np.log2(work[i][1]) for i in iso])
+        ys = np.array(list(iso.values()))
+        order = np.argsort(xs)
+
+        def isolated(i):
+            return float(np.interp(np.log2(work[i][1]), xs[order], ys[order]))
+
+        for load in a.loads:
+            rate = load * cap
+            arr = np.cumsum(np.random.default_rng(1234).exponential(1.0 / rate, size=len(work)))
+            t = time.perf_counter()
+            lat = run_stream(srv, work, arr)
+            wall = time.perf_counter() - t
+            ratio = np.array([lat[i] / isolated(i) for i in range(len(work))])
+            out["loads"][f"{load:g}"] = {
+                "rate_jobs_per_s": rate, "p50_latency_s": float(np.percentile(lat, 50)),
+                "p99_latency_s": float(np.percentile(lat, 99)),
+                "p50_over_isolated": float(np.percentile(ratio, 50)),
+                "p99_over_isolated": float(np.percentile(ratio, 99)),
+                "particle_steps_per_s": psteps / wall}
+        out["isolated_sample"] = {"jobs": len(iso), "median_s": float(np.median(ys))}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -82,6 +82,19 @@ def test_fp32_results_independent_of_launch_shape():
     assert a["counts"][L.C_STEPS].min() == 120_000
 
 
+def test_fp32_launch_boundaries_on_the_barrier_flank():
+    # Start on the barrier flank (nonzero force) and cut the run into very
+    # short launches: the hot state carried across a launch boundary or a
+    # refill (force, band, countdown) must give the same trajectory.
+    p = quick(steps=24_000, freq=20, x0=-0.3)
+    with ldp.Context(0) as c1, ldp.Context(0) as c2:
+        set_shape(c1, 256, 0, 1 << 15)
+        set_shape(c2, 64, 1, 37)
+        a = run(c1, p, ldp.PREC_FP32_BATCHED, lanes=256)
+        b = run(c2, p, ldp.PREC_FP32_BATCHED, lanes=256)
+    same(a, b)
+
+
 def test_fp32_double_and_underdamped_independent_of_launch_shape():
     for p in (double(), quick(overdamped=0), double(overdamped=0)):
         with ldp.Context(0) as c1, ldp.Context(0) as c2:
