@@ -1,0 +1,105 @@
+"""Autotuner of the FP32 batched launch shape; writes tuning.json.
+
+For each model type (single / double barrier x over- / underdamped) it runs a
+fixed synthetic workload under every candidate shape -- threads per block,
+resident blocks per SM, step pairs per slot and launch (steps per launch =
+2 x pairs) -- timing the persistent launches with device events, and keeps
+the fastest.  Trajectories per thread are one by design (a slot owns one
+trajectory; the resident slots are blocks_per_sm x block x SMs), so the
+per-thread count is not a free parameter here.  The shape lives in a
+context and is fixed at its first FP32 job; ``_tune.apply_tuned(ctx, model)``
+applies the committed result.
+
+    python -m langevindynamicsforpcp_b200.autotune [--out path] [--steps N]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import (Context, Job, MODEL_DOUBLE, MODEL_SINGLE, PREC_FP32_BATCHED, params_from_inp_text, submit_batch)
+from . import _tune
+from .serve import COMMON, DOUBLE, SINGLE
+
+MODELS = {"single_over": (False, True), "single_under": (False, False),
+          "double_over": (True, True), "double_under": (True, False)}
+CANDIDATES = [(block, bps, pb) for block in (128, 256) for bps in (0,) for pb in (4096, 16384, 65536)]
+
+
+def workload(model: str, steps: int, njobs: int, ntraj: int):
+    """njobs jobs of the model: CuIDB geometry, H_low in {2, 3, 4, 5},
+    flip rate logU[1e-2, 1e2], gamma 1, drawn with default_rng(1234)."""
+    dbl, over = MODELS[model]
+    rng = np.random.default_rng(1234)
+    out = []
+    for _ in range(njobs):
+        h = float(rng.choice([2.0, 3.0, 4.0, 5.0]))
+        k = float(10 ** rng.uniform(-2, 2))
+        text = COMMON.format(over="true" if over else "false", gamma=1.0, steps=steps, freq=20, tau=1.0 / k,
+                             seed=1234)
+        text += DOUBLE.format(mid=1.7 * h, high=3.6 * h, low=h) if dbl else SINGLE.format(high=3.6 * h, low=h)
+        out.append(params_from_inp_text(text, MODEL_DOUBLE if dbl else MODEL_SINGLE))
+    return out, ntraj
+
+
+def time_shape(shape, params, ntraj, repeat: int) -> float:
+    """Best integration time (ms) of the batch over `repeat` runs."""
+    block, bps, pb = shape
+    best = float("inf")
+    with Context(0) as ctx:
+        _tune.set_fp32_shape(ctx, block=block, blocks_per_sm=bps, pair_budget=pb)
+        for r in range(repeat + 1):
+            jobs = [Job(ctx, p, lanes=ntraj, precision=PREC_FP32_BATCHED, job_id=i) for i, p in enumerate(params)]
+            submit_batch(ctx, jobs)
+            for j in jobs:
+                j.wait()
+            ms = jobs[0].timing()["integrate_ms"]
+            for j in jobs:
+                j.close()
+            if r:                      # the first run warms up
+                best = min(best, ms)
+        grid = _tune.get_fp32_shape(ctx)["grid"]
+    return best, grid
+
+
+def main(argv=None):
+    here = os.path.dirname(os.path.abspath(__file__))
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(here, "tuning.json"))
+    ap.add_argument("--steps", type=int, default=24000)
+    ap.add_argument("--jobs", type=int, default=4)
+    ap.add_argument("--ntraj", type=int, default=65536)
+    ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--models", nargs="+", default=list(MODELS))
+    a = ap.parse_args(argv)
+    import torch
+    result = {"device": torch.cuda.get_device_name(0),
+              "created": time.strftime("%Y-%m-%d %H:%M:%S"),
+              "workload": f"{a.jobs} jobs x {a.ntraj} trajectories x {a.steps} steps per model "
+                          f"(CuIDB geometry, H_low in {{2,3,4,5}}, flip rate logU[1e-2,1e2])",
+              "trajectories_per_thread": 1, "shapes": {}, "trials": []}
+    for model in a.models:
+        params, ntraj = workload(model, a.steps, a.jobs, a.ntraj)
+        psteps = a.jobs * ntraj * a.steps
+        best = None
+        for shape in CANDIDATES:
+            ms, grid = time_shape(shape, params, ntraj, a.repeat)
+            rate = psteps / (ms * 1e-3)
+            result["trials"].append({"model": model, "block": shape[0], "blocks_per_sm": shape[1],
+                                     "pair_budget": shape[2], "grid": grid, "ms": ms, "steps_per_s": rate})
+            if best is None or rate > best[1]:
+                best = (shape, rate, grid)
+        (block, bps, pb), rate, grid = best
+        result["shapes"][model] = {"block": block, "blocks_per_sm": bps, "pair_budget": pb, "ring_slots": 64,
+                                   "grid": grid, "steps_per_s": rate}
+        print(json.dumps({"model": model, **result["shapes"][model]}), flush=True)
+    with open(a.out, "w") as f:
+        json.dump(result, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
