@@ -6,7 +6,7 @@ path on one B200 (and N replicas), on the "precision" workload:
   gamma 1, kT 1, dt 1e-5; per job H_low drawn from {2,3,4,5} with the high
   barrier 3.6 x H_low and the flip rate k log-uniform in [1e-2, 1e2]
   (TAU = 1/k), drawn with numpy default_rng(1234); FPT/TPT/FPTCG statistics
-  on; 60000 steps per trajectory with frames every 20 steps (3001 frames,
+  on; 300000 steps per trajectory (3 time units) with frames every 100 steps (3001 frames,
   MSD on the reference's log-spaced lags).  Synthetic inputs: the reference
   ships no dataset.
 
@@ -37,7 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 OPS_PER_STEP = 70   # lane instructions per overdamped single-barrier step (algorithmic count)
-NJOBS, NTRAJ, NSTEPS, FREQSAVE = 16, 65536, 60000, 20
+NJOBS, NTRAJ, NSTEPS, FREQSAVE = 16, 65536, 300000, 100
+# DRAM bytes per particle-step of the persistent kernel: 0.434 B measured by
+# ncu with frames every 20 steps (8 B per frame = 0.40 B per step of it);
+# scaled to this workload's frame interval.
+DRAM_BYTES_PER_STEP = 0.434 - 8.0 / 20 + 8.0 / FREQSAVE
 
 
 def workload_params(ldp, job0=0, njobs=NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE):
@@ -125,6 +129,39 @@ def run_batch(ldp, ctx, params, precision, job_id0=0):
     return jobs
 
 
+def job_summary(job):
+    """MSD curve and renewal-event means of a finished job (host copies)."""
+    from langevindynamicsforpcp_b200 import _lib as L
+    r = job.results(frames=False, ticks=False)
+    lags, msd = job.msd()
+    c, s = r["counts"], r["sums"]
+    out = {"msd": msd, "lags": lags}
+    for name, ci, si in (("fpt", L.C_FPT, L.S_FPT), ("fpt2", L.C_FPT2, L.S_FPT2), ("tpt", L.C_TPT, L.S_TPT)):
+        n = float(c[ci].sum())
+        per = np.where(c[ci] > 0, s[si] / np.maximum(c[ci], 1), np.nan)
+        out[name] = (float(s[si].sum()) / n if n else None, int(n),
+                     float(np.nanstd(per) / np.sqrt(np.sum(c[ci] > 0))) if n else None)
+    return out
+
+
+def compare_summaries(a, b):
+    """FP32 batched job 0 against the FP64 plain run of the same job (same
+    parameters, seed and job id): relative differences, with the standard
+    error of the FP64 mean for scale (the two runs share their noise but
+    not every trajectory, so the difference includes sampling noise)."""
+    out = {}
+    ok = b["msd"] > 0
+    rel = np.abs(a["msd"][ok] - b["msd"][ok]) / b["msd"][ok]
+    out["msd_max_rel_err"] = float(rel.max())
+    out["msd_mean_rel_err"] = float(rel.mean())
+    for k in ("fpt", "fpt2", "tpt"):
+        (ma, na, _), (mb, nb, se) = a[k], b[k]
+        if ma is not None and mb is not None:
+            out[k] = {"fp32_mean": ma, "fp64_mean": mb, "rel_err": abs(ma - mb) / mb, "fp64_rel_se": se / mb if se else None,
+                      "events_fp32": na, "events_fp64": nb}
+    return out
+
+
 def cpu_baseline_worker(args):
     seed, traj_begin, ntraj, nsteps = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -161,6 +198,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nsteps", type=int, default=None, help="steps per trajectory (profiling cases)")
     ap.add_argument("--njobs", type=int, default=None, help="jobs per batch (profiling cases)")
+    ap.add_argument("--freqsave", type=int, default=None, help="steps between frames (profiling cases)")
     ap.add_argument("--ntraj", type=int, default=None, help="trajectories per job (profiling cases)")
     args = ap.parse_args()
 
@@ -182,18 +220,21 @@ def main():
     import langevindynamicsforpcp_b200 as ldp
     from langevindynamicsforpcp_b200 import _tune
 
-    global NJOBS, NTRAJ, NSTEPS
+    global NJOBS, NTRAJ, NSTEPS, FREQSAVE, DRAM_BYTES_PER_STEP
     if args.small:
         NJOBS, NTRAJ = 2, 16384
     if args.nsteps:
         NSTEPS = args.nsteps
     if args.njobs:
         NJOBS = args.njobs
+    if args.freqsave:
+        DRAM_BYTES_PER_STEP += 8.0 / args.freqsave - 8.0 / FREQSAVE
+        FREQSAVE = args.freqsave
     if args.ntraj:
         NTRAJ = args.ntraj
     ctx = ldp.Context(local)
     shape = _tune.apply_tuned(ctx, "single_over")
-    params = workload_params(ldp, 0, NJOBS, nsteps=NSTEPS)
+    params = workload_params(ldp, 0, NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE)
     job_id0 = rank * 1000   # replicas integrate different trajectories
     psteps = NJOBS * NTRAJ * NSTEPS
 
@@ -225,6 +266,7 @@ def main():
             # one job after the other: the last one ends post_ms after it
             msd_ms.append(max(j.timing()["msd_ms"] for j in jobs))
             launches += sum(j.timing()["launches"] for j in jobs)
+            acc32 = job_summary(jobs[0])
             for j in jobs:
                 j.close()
     clocks = clk.summary()
@@ -250,7 +292,9 @@ def main():
             ctx.mark(3)
             if it >= args.warmup:
                 t64.append(ctx.elapsed_ms(2, 3))
+            acc64 = job_summary(j)
     fp64_value = NTRAJ * NSTEPS / (sum(t64) / len(t64) * 1e-3)
+    accuracy = compare_summaries(acc32, acc64)
 
     # ---- end to end through the C ABI: host params in, host results out ----
     e2e_t = []
@@ -291,7 +335,11 @@ def main():
     achieved = psteps * OPS_PER_STEP / (kms * 1e-3) / 1e9
     fclk = clocks.get("sm_mhz") or fmax
     roofline = {"bound": "issue", "achieved": achieved, "peak": peak_issue, "unit": "Ginstr/s",
-                "frac": achieved / peak_issue, "traffic": None,
+                "frac": achieved / peak_issue, "traffic": DRAM_BYTES_PER_STEP * psteps,
+                "traffic_scope": "DRAM bytes of the persistent kernel per bench step (all its launches): "
+                                 f"{DRAM_BYTES_PER_STEP} B per particle-step from the ncu capture in "
+                                 "profiles/fp32_persistent_kernel__single_over_113664traj_24000steps.md, "
+                                 "scaled by particle-steps and frame interval; algorithmic bytes: the frames, 8 B per FREQSAVE steps",
                 "kernel": "fp32_persistent_kernel<single, overdamped>",
                 "ops_per_step": OPS_PER_STEP, "kernel_ms": kms,
                 "peak_basis": f"{sms} SMs x 128 lanes x sm_max_mhz {fmax:g} (MEASURED_PEAKS.json)",
@@ -303,15 +351,17 @@ def main():
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "precision: 16 single-barrier jobs x 65536 trajectories, dt 1e-5, 60000 steps, "
-                                   "3001 frames, per-job H in {2,3,4,5}, high 3.6H, flip rate logU[1e-2,1e2]",
+            "config": {"workload": f"precision: {NJOBS} single-barrier jobs x {NTRAJ} trajectories, dt 1e-5, "
+                                   f"{NSTEPS} steps, {NSTEPS // FREQSAVE + 1} frames, per-job H in {{2,3,4,5}}, "
+                                   "high 3.6H, flip rate logU[1e-2,1e2]",
                        "trajectories": NJOBS * NTRAJ * world, "steps_per_trajectory": NSTEPS,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before each step; "
                                                                  "frames 25 GB per step",
                        "fp32_shape": shape_used, "tuned": bool(shape)},
             "fp64_plain": {"value": fp64_value, "unit": "particle-steps/s",
-                           "sample": "job 0 alone (65536 trajectories x 60000 steps)"},
+                           "sample": f"job 0 alone ({NTRAJ} trajectories x {NSTEPS} steps)"},
             "fp32_over_fp64": value / world / fp64_value,
+            "accuracy_vs_fp64": accuracy,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches / max(1, args.steps)),

@@ -274,8 +274,10 @@ void        ldp_job_destroy(ldp_job *job);
 /* Serving loop (continuous batching of FP32 batched jobs).  No counterpart
  * in the reference, which runs one .inp per MPI process (src/mpiKernel.cpp).
  * Requests are submitted at any time (ldp_server_submit is thread-safe);
- * each ldp_server_step admits queued jobs in arrival order while their
- * device footprint fits hbm_budget, keeps short persistent launches in
+ * each ldp_server_step admits queued jobs, oldest first, while their device
+ * footprint fits hbm_budget (later jobs that fit may pass a waiting one for
+ * at most 0.25 s), publishes their trajectories shortest-remaining-job
+ * first in chunks, keeps short persistent launches in
  * flight for every model type with work, and finishes jobs whose
  * trajectories all retired.  Jobs joining mid-run share the launches with
  * those already running; every result equals that of the job run alone.
@@ -286,7 +288,7 @@ typedef enum {
 } ldp_server_state;
 typedef struct ldp_server_opts {
     int64_t hbm_budget;     /* bytes of job arenas resident at once (0: 80% of free memory) */
-    int64_t pair_budget;    /* step pairs per slot per persistent launch (0: 2048)           */
+    int64_t pair_budget;    /* step pairs per slot per persistent launch (0: 1024)           */
     int32_t max_inflight;   /* persistent launches in flight per model type (1..16)         */
     int32_t pad;
 } ldp_server_opts;
@@ -301,6 +303,9 @@ ldp_status  ldp_server_submit(ldp_server *s, const ldp_params *p, const ldp_job_
 ldp_status  ldp_server_step(ldp_server *s, int *ndone);
 /* state: ldp_server_state; latency_s: submission to done (0 until done). */
 ldp_status  ldp_server_poll(ldp_server *s, uint64_t ticket, int *state, double *latency_s);
+/* Seconds from submission to admission, to all trajectories retired, and to
+ * done (-1 for a stage not reached yet): where a job's latency went. */
+ldp_status  ldp_server_job_times(ldp_server *s, uint64_t ticket, double times[3]);
 /* The finished job (owned by the server until ldp_server_release). */
 ldp_status  ldp_server_job(ldp_server *s, uint64_t ticket, ldp_job **job);
 ldp_status  ldp_server_release(ldp_server *s, uint64_t ticket);

@@ -2,12 +2,13 @@
 //
 // Requests (.inp parameter sets with job options) are submitted at any time
 // and from any thread; each step of the loop
-//  1. admits queued jobs in arrival order while their device footprint fits
-//     the memory budget (a job larger than the whole budget is admitted
-//     alone), allocating their arena and registering them with the work
-//     queue of their model type;
+//  1. admits queued jobs while their device footprint fits the memory
+//     budget, oldest first, letting later jobs that fit pass one that does
+//     not for at most kBypassWindow (a job larger than the whole budget is
+//     admitted alone), allocating their arena and registering them with the
+//     work queue of their model type;
 //  2. publishes admitted jobs' trajectories to the queue in chunks, keeping
-//     about one wave of slots' worth of unclaimed work queued and always
+//     about half a wave of slots' worth of unclaimed work queued and always
 //     publishing next for the job with the fewest unpublished trajectories
 //     (shortest remaining first): a small job that arrives while large ones
 //     run starts within one chunk, instead of after every earlier job;
@@ -43,6 +44,8 @@
 
 namespace {
 
+constexpr double kBypassWindow = 0.25;   // seconds the oldest pending job may be passed
+
 double now_s() {
     using namespace std::chrono;
     return duration<double>(steady_clock::now().time_since_epoch()).count();
@@ -55,7 +58,7 @@ struct Entry {
     int state = LDP_SRV_QUEUED;
     int type = -1;
     uint64_t gen_admit = 0;          // remaining-counter copies issued before admission
-    double t_submit = 0, t_admit = 0, t_done = 0;
+    double t_submit = 0, t_admit = 0, t_ready = 0, t_done = 0;
     cudaEvent_t fin = nullptr;       // post-processing done
 };
 
@@ -104,7 +107,7 @@ extern "C" void ldp_server_opts_default(ldp_server_opts* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->hbm_budget = 0;        // 80% of the free device memory at creation
-    o->pair_budget = 2048;    // step pairs per slot per launch
+    o->pair_budget = 1024;    // step pairs per slot per launch
     o->max_inflight = 2;
 }
 
@@ -122,14 +125,19 @@ extern "C" ldp_status ldp_server_create(ldp_ctx* ctx, const ldp_server_opts* o, 
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = opts.hbm_budget ? (size_t)opts.hbm_budget : (size_t)(0.8 * (double)free_b);
-    s->pair_budget = opts.pair_budget ? (uint32_t)opts.pair_budget : 2048u;
+    s->pair_budget = opts.pair_budget ? (uint32_t)opts.pair_budget : 1024u;
     s->max_inflight = opts.max_inflight;
-    cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    // Post-processing runs at the highest stream priority: the persistent
+    // launches fill every SM, and a finished job's MSD blocks should take
+    // the SMs the next launch boundary frees before new persistent blocks.
+    int lo_prio = 0, hi_prio = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    cudaError_t e = cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi_prio);
     for (int t = 0; t < 4 && e == cudaSuccess; ++t) {
         // the queue's counters, then its claimed-items count
         e = cudaMallocHost((void**)&s->h_rem[t], sizeof(unsigned long long) * (ldp::kFp32MaxJobs + 1));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->rem_ev[t], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->qs[t], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->qs[t], cudaStreamNonBlocking, lo_prio);
     }
     if (e != cudaSuccess) {
         ldp_server_destroy(s);
@@ -172,16 +180,27 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
     cudaStream_t st = ctx->stream;
     int done = 0;
 
-    // 1. admission, in arrival order, by footprint
-    for (;;) {
+    // 1. admission by footprint, oldest first; a later job that fits may
+    //    pass one that does not, unless the oldest pending job has waited
+    //    longer than the bypass window (then it is admitted next).
+    const double t_now = now_s();
+    for (size_t i = 0;;) {
         Entry* en = nullptr;
+        size_t pos = 0;
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            if (s->pending.empty()) break;
-            en = s->pending.front();
+            if (i >= s->pending.size()) break;
+            Entry* c = s->pending[i];
             const bool idle = s->running.empty() && s->finishing.empty();
-            if (!idle && s->in_use + en->bytes > s->budget) break;
-            s->pending.pop_front();
+            if (idle || s->in_use + c->bytes <= s->budget) {
+                en = c;
+                pos = i;
+                s->pending.erase(s->pending.begin() + (std::ptrdiff_t)i);
+            } else {
+                if (i == 0 && t_now - c->t_submit > kBypassWindow) break;
+                ++i;
+                continue;
+            }
         }
         ldp_job* job = en->job;
         if (ldp_job_arena(job, true) == 0) {
@@ -194,7 +213,7 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
                 continue;
             }
             std::lock_guard<std::mutex> lk(s->mu);
-            s->pending.push_front(en);
+            s->pending.insert(s->pending.begin() + (std::ptrdiff_t)pos, en);
             break;
         }
         job->launches = 0;
@@ -223,7 +242,7 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         const int64_t wave = ldp::fp32_nslots(ctx, t);
         const unsigned long long pub = ldp::fp32_published(ctx, t);
         int64_t backlog = (int64_t)(pub - std::min(pub, s->head_seen[t]));
-        while (backlog < wave) {
+        while (backlog < wave / 2) {
             Entry* best = nullptr;
             int64_t best_left = 0;
             for (Entry* en : s->running) {
@@ -232,7 +251,7 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
                 if (left > 0 && (!best || left < best_left)) { best = en; best_left = left; }
             }
             if (!best) break;
-            const int64_t chunk = std::min<int64_t>(best_left, std::max<int64_t>(wave - backlog, 1024));
+            const int64_t chunk = std::min<int64_t>(best_left, std::max<int64_t>(wave / 2 - backlog, 1024));
             const int e = ldp::fp32_publish_range(best->job, chunk, s->qs[t]);
             if (e) return fail(s, "publication", (cudaError_t)e);
             backlog += chunk;
@@ -280,6 +299,7 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
                 en->fin = s->get_event();
                 cudaEventRecord(en->fin, s->side);
                 en->state = LDP_SRV_FINISHING;
+                en->t_ready = now_s();
                 en->job->fp32_phase = 2;
                 s->finishing.push_back(en);
                 s->running[i] = s->running.back();
@@ -329,6 +349,19 @@ extern "C" ldp_status ldp_server_poll(ldp_server* s, uint64_t ticket, int* state
     *state = en->state;
     if (latency_s) *latency_s = (en->state == LDP_SRV_DONE || en->state == LDP_SRV_FAILED) ? en->t_done - en->t_submit
                                                                                           : 0.0;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_job_times(ldp_server* s, uint64_t ticket, double* times) {
+    if (!s || !times) return LDP_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return LDP_ERR_INVALID;
+    const Entry* en = it->second;
+    auto rel = [&](double t) { return t > 0.0 ? t - en->t_submit : -1.0; };
+    times[0] = rel(en->t_admit);
+    times[1] = rel(en->t_ready);
+    times[2] = rel(en->t_done);
     return LDP_OK;
 }
 

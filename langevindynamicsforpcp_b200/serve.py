@@ -71,7 +71,7 @@ DOUBLE = ("BARRIERHEIGHTS0 {mid!r} {low!r}\nBARRIERHEIGHTS1 {high!r} {low!r}\nBA
 class Server:
     """The library's serving loop (ldp_server_create ... ldp_server_destroy)."""
 
-    def __init__(self, ctx: Context, hbm_budget: int = 0, pair_budget: int = 2048, max_inflight: int = 2):
+    def __init__(self, ctx: Context, hbm_budget: int = 0, pair_budget: int = 1024, max_inflight: int = 2):
         self.ctx = ctx
         o = L.ServerOpts()
         L.lib().ldp_server_opts_default(C.byref(o))
@@ -97,6 +97,12 @@ class Server:
         st, lat = C.c_int(0), C.c_double(0)
         _check(L.lib().ldp_server_poll(self.handle, ticket, C.byref(st), C.byref(lat)), self.ctx)
         return st.value, lat.value
+
+    def times(self, ticket: int):
+        """(admitted, trajectories retired, done), seconds after submission."""
+        t = (C.c_double * 3)()
+        _check(L.lib().ldp_server_job_times(self.handle, ticket, t), self.ctx)
+        return tuple(t)
 
     def job(self, ticket: int) -> Job:
         h = C.c_void_p()
@@ -146,10 +152,11 @@ def serving_workload(n: int, seed: int = 1234, exp_lo: float = 10, exp_hi: float
     return out
 
 
-def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 900.0):
+def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 900.0, stages=None):
     """Submits work[i] at time arrivals[i] (seconds from now), drives the
     loop until every job is done; returns per-job latency (submission to
-    done, seconds).  on_done(i, job) is called before each job is released."""
+    done, seconds).  on_done(i, job) is called before each job is released;
+    stages (an n x 3 array) receives each job's server.times()."""
     n = len(work)
     lat = np.full(n, np.nan)
     tickets = {}
@@ -171,6 +178,8 @@ def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 
                     if st == L.SRV_FAILED:
                         raise RuntimeError(f"job {i} failed: {server.ctx.last_error()}")
                     lat[i] = l
+                    if stages is not None:
+                        stages[i] = server.times(t)
                     if on_done:
                         on_done(i, server.job(t))
                     server.release(t)
@@ -199,34 +208,55 @@ def main(argv=None):
         makespan = time.perf_counter() - t
         cap = len(work) / makespan
         out["capacity"] = {"jobs_per_s": cap, "particle_steps_per_s": psteps / makespan, "makespan_s": makespan}
-        # isolated solve times of a sample spanning the sizes, per type
+        # isolated solve time: each job alone in the server (every job when
+        # --isolated-sample covers them all, else a sample interpolated by
+        # trajectory count within the job's model type)
         rng = np.random.default_rng(7)
-        sample = rng.choice(len(work), size=min(a.isolated_sample, len(work)), replace=False)
+        n_iso = min(a.isolated_sample, len(work))
+        sample = range(len(work)) if n_iso == len(work) else rng.choice(len(work), size=n_iso, replace=False)
         iso = {}
         for i in sample:
-            l = run_stream(srv, [work[i]], [0.0])
-            iso[int(i)] = float(l[0])
-        xs = np.array([np.log2(work[i][1]) for i in iso])
-        ys = np.array(list(iso.values()))
-        order = np.argsort(xs)
+            iso[int(i)] = float(run_stream(srv, [work[i]], [0.0])[0])
+        kind = lambda i: (work[i][2]["double"], work[i][2]["overdamped"])
 
         def isolated(i):
-            return float(np.interp(np.log2(work[i][1]), xs[order], ys[order]))
+            if i in iso:
+                return iso[i]
+            same = [j for j in iso if kind(j) == kind(i)] or list(iso)
+            xs = np.array([np.log2(work[j][1]) for j in same])
+            ys = np.array([iso[j] for j in same])
+            o = np.argsort(xs)
+            return float(np.interp(np.log2(work[i][1]), xs[o], ys[o]))
 
         for load in a.loads:
             rate = load * cap
             arr = np.cumsum(np.random.default_rng(1234).exponential(1.0 / rate, size=len(work)))
             t = time.perf_counter()
-            lat = run_stream(srv, work, arr)
+            stg = np.zeros((len(work), 3))
+            lat = run_stream(srv, work, arr, stages=stg)
             wall = time.perf_counter() - t
             ratio = np.array([lat[i] / isolated(i) for i in range(len(work))])
+            size = np.array([np.log2(w[1]) for w in work])
+            classes = {}
+            for name, lo_, hi_ in (("2^10-2^13", 0, 13), ("2^13-2^16", 13, 16), ("2^16-2^18", 16, 99)):
+                m = (size >= lo_) & (size < hi_)
+                if m.any():
+                    classes[name] = {"jobs": int(m.sum()), "p50_over_isolated": float(np.percentile(ratio[m], 50)),
+                                     "p99_over_isolated": float(np.percentile(ratio[m], 99))}
             out["loads"][f"{load:g}"] = {
+                "by_trajectory_count": classes,
                 "rate_jobs_per_s": rate, "p50_latency_s": float(np.percentile(lat, 50)),
                 "p99_latency_s": float(np.percentile(lat, 99)),
                 "p50_over_isolated": float(np.percentile(ratio, 50)),
                 "p99_over_isolated": float(np.percentile(ratio, 99)),
-                "particle_steps_per_s": psteps / wall}
-        out["isolated_sample"] = {"jobs": len(iso), "median_s": float(np.median(ys))}
+                "particle_steps_per_s": psteps / wall,
+                "p99_stage_s": {"queued": float(np.percentile(stg[:, 0], 99)),
+                                "integrating": float(np.percentile(stg[:, 1] - stg[:, 0], 99)),
+                                "post_processing": float(np.percentile(stg[:, 2] - stg[:, 1], 99))},
+                "worst_jobs": [{"job": int(i), "ntraj": work[i][1], "latency_s": float(lat[i]),
+                                "isolated_s": isolated(int(i)), "stages_s": [float(x) for x in stg[i]]}
+                               for i in np.argsort(-(lat / np.array([isolated(k) for k in range(len(work))])))[:4]]}
+        out["isolated"] = {"jobs": len(iso), "median_s": float(np.median(list(iso.values())))}
     print(json.dumps(out))
 
 
