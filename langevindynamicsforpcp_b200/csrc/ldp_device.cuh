@@ -6,17 +6,24 @@
 // (src/RANDOMNUMBER.cpp:70-340; streams created at
 // src/langevinDynamicsSingleBarrier.h:1288-1290); the draw points stay where
 // the reference has them:
-//   TAG_STEP    a = (step-1)>>1: words 0,1 -> Box-Muller pair (cosine branch
-//               for odd steps, sine branch for even steps); words 2,3 -> the
-//               per-step flip uniform of the odd / even step.
+//   TAG_STEP    a = (step-1)>>2: words 0,1 -> Box-Muller pair of steps 4a+1
+//               (cosine branch) and 4a+2 (sine branch); words 2,3 -> pair of
+//               steps 4a+3 and 4a+4.
 //   TAG_INIT    a = 0: word 0 -> initial barrier state, words 1,2 ->
 //               Box-Muller pair (v0, R0).
 //   TAG_CATCHUP a = step: words 0,1 -> 64-bit uniform of the lazy catch-up
 //               flip on entering a cell (S.h:2025-2068).
 //   TAG_CELL    a = cell key: word 0 -> state of a never-visited cell
 //               (BarrierStatus::Initialize, S.h:78-96).
-//   TAG_REFINE  a = step: word 0 -> low 32 bits of the per-step flip uniform,
-//               drawn only when the high word ties the threshold.
+//   TAG_FLIP    a = step: words 0,1 -> 64-bit uniform of the waiting time to
+//               the current barrier's next flip, drawn at step 0 and at every
+//               step whose barrier state or barrier changed.
+//
+// The reference flips the current barrier with probability p each step
+// (S.h:2010-2015); those flips form a Bernoulli process, so the steps
+// between them are geometric, and drawing the waiting time once per flip
+// (or per barrier change: the process is memoryless) gives the same process
+// while each step needs only its Gaussian.
 //
 // The FP64 functions below evaluate a fixed operation sequence with explicit
 // fma() so that the FP64 device path is bit-identical to a host evaluation
@@ -26,7 +33,7 @@
 
 namespace ldp {
 
-enum : uint32_t { TAG_STEP = 0, TAG_INIT = 1, TAG_CATCHUP = 2, TAG_CELL = 3, TAG_REFINE = 4 };
+enum : uint32_t { TAG_STEP = 0, TAG_INIT = 1, TAG_CATCHUP = 2, TAG_CELL = 3, TAG_FLIP = 4 };
 
 struct Words { uint32_t w0, w1, w2, w3; };
 
@@ -156,6 +163,18 @@ __device__ __forceinline__ double expm1_f64(double x) {
     if (k == 0.0) return e;
     const double s = ldexp(1.0, (int)k);
     return fma(s, e, s - 1.0);
+}
+
+// Steps from the current one to the next flip of a barrier that flips with
+// probability p per step, ln1m = log(1 - p): W = 1 + floor(ln U / ln(1-p))
+// for U in (0, 1] from the 64-bit word pair (geometric, P(W = k) =
+// (1-p)^(k-1) p); UINT64_MAX when the barrier never flips.
+__device__ __forceinline__ uint64_t flip_wait(uint32_t hi, uint32_t lo, double ln1m) {
+    if (!(ln1m < 0.0)) return 0xffffffffffffffffull;
+    const double u = ((double)(((uint64_t)hi << 32) | lo) + 1.0) * 0x1p-64;
+    const double q = log_f64(u) / ln1m;
+    if (!(q < 0x1p62)) return 0xffffffffffffffffull;
+    return 1ull + (uint64_t)floor(q);
 }
 
 __device__ __forceinline__ uint64_t prob_to_u64(double p) {

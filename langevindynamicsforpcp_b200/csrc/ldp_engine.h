@@ -35,6 +35,7 @@ struct KConst {
     double Hd[2][2], sN[2][2], sP[2][2], iN[2][2], iP[2][2];
     double c_drift, sig_r, invM, hdt, expg, sig_v, mhalf, sig_v0;
     uint64_t T_eq, T_as[2];
+    double ln1m[2];          // log(1 - per-step flip probability) by state; 0: never flips
     double a_lap, c_lap[2], p_first, p_cell0;
     uint64_t nsteps, freq_save, step_cap;
     int64_t nframe, tick_cap;
@@ -51,6 +52,7 @@ struct TrajState {
     int32_t *state, *lb, *bits;
     double *fpt_last, *fpt2_last, *tpt_last, *tpt2_last;
     int64_t *init_idx0, *init_idx1, *idx2_0, *idx2_1, *tpt2_well, *wt_tick;
+    int64_t* nflip;     // step of the current barrier's next flip
     double *cg_last;    // [LDP_MAX_CG][n]
     int64_t *cg_well;   // [LDP_MAX_CG][n]
     int64_t *counts;    // [LDP_NCOUNT][n]

@@ -70,7 +70,8 @@ struct RareSm {
     // Lane state the hot loop hands to the general step and takes back, and
     // the lane state only the general step uses.
     float xp[kMaxBlock], rv[kMaxBlock], F[kMaxBlock], lo[kMaxBlock], hi[kMaxBlock], c1[kMaxBlock];
-    uint32_t thi[kMaxBlock], traj[kMaxBlock];
+    uint32_t traj[kMaxBlock];
+    long long nflip[kMaxBlock];   // step of the current barrier's next flip
     int32_t left[kMaxBlock], job[kMaxBlock], cell[kMaxBlock], state[kMaxBlock], sw[kMaxBlock];
 };
 
@@ -80,8 +81,13 @@ __device__ __forceinline__ void red_add(int64_t* p, int64_t v) {
 
 __device__ __forceinline__ int fkey(bool dbl, int cell, int lb) { return dbl ? cell * 2 + lb : cell; }
 
-__device__ __forceinline__ uint32_t thi_of(const JobF& J, int st) {
-    return (uint32_t)((J.eq ? J.T_eq : J.T_as[st]) >> 32);
+// Step of the next flip of a barrier now in state st, scheduled at step s
+// (words of TAG_FLIP at a = s; geometric waiting time, FP64 as in the FP64
+// path, so both precisions schedule the same flips from the same history).
+__device__ __forceinline__ long long next_flip(const JobF& J, uint32_t traj, uint64_t s, int st) {
+    const Words w = philox_at(s, traj, TAG_FLIP, J.key0, J.key1);
+    const uint64_t wt = flip_wait(w.w0, w.w1, J.ln1m[st]);
+    return (wt >= 0x7fffffffffffffffull - s) ? 0x7fffffffffffffffll : (long long)(s + wt);
 }
 
 // Uniform in (0, 1): the high 23 bits of w as a mantissa, offset by 2^-24.
@@ -268,6 +274,7 @@ __device__ __noinline__ void f_start(const JobF* Jp, longlong2* ring, int64_t ns
     sm->cgw[t] = INT32_MIN;
     sm->fidx[t] = 1;
     sm->nxf[t] = (!J.fp_mode && J.freq_save) ? (long long)J.freq_save : INT64_MAX;
+    sm->nflip[t] = next_flip(J, traj, 0, st);
     sm->fpt[t] = sm->fpt2[t] = sm->tpt[t] = sm->tpt2[t] = 0;
     sm->cstamp[t] = 0;
     sm->sc1[t] = 0;
@@ -311,9 +318,11 @@ __device__ __noinline__ int64_t f_resolve(const int64_t* range_end, const int32_
     return range_first[lo] + (idx - begin);
 }
 
-// Steps from step s to the next frame (step nxf) or the last step.
-__device__ __forceinline__ int steps_to_special(const JobF& J, uint64_t s, long long nxf) {
-    const uint64_t e = (uint64_t)nxf < J.nsteps ? (uint64_t)nxf : J.nsteps;
+// Steps from step s to the next frame (step nxf), flip (step nf) or the
+// last step.
+__device__ __forceinline__ int steps_to_special(const JobF& J, uint64_t s, long long nxf, long long nf) {
+    uint64_t e = (uint64_t)nxf < J.nsteps ? (uint64_t)nxf : J.nsteps;
+    e = (uint64_t)nf < e ? (uint64_t)nf : e;
     const uint64_t d = e - s;
     return (int)(d < (uint64_t)kLeftMax ? d : (uint64_t)kLeftMax);
 }
@@ -336,13 +345,13 @@ __device__ __forceinline__ void retire_lane(const JobF& J, unsigned long long* r
     f_retire(&J, retired, sm.traj[t], done, sc1, sm.cell[t], xp, OVER ? 0.0f : v, state, flags);
 }
 
-// The general step s of one lane (position already advanced, flip word fw):
+// The general step s of one lane (position already advanced):
 // the FP64 step order of ldp_fp64.cu from the index update on.  Out of line,
 // on the lane state in shared memory, so that the hot loop's registers do
 // not carry its working set.
 template <bool DBL, bool OVER>
 __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, RareSm* smp, int t, int64_t slot,
-                                          uint64_t s, uint32_t fw) {
+                                          uint64_t s) {
     RareSm& sm = *smp;
     const SlotsDev& S = *Sp;
     const float kInf = __int_as_float(0x7f800000);
@@ -363,7 +372,6 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
         sm.job[t] = -1;
         sm.lo[t] = -kInf;
         sm.hi[t] = kInf;
-        sm.thi[t] = 0;
         sm.F[t] = 0.f;
         sm.left[t] = kLeftMax;
     };
@@ -511,7 +519,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
         return done;
     };
 
-    if (xp > lo && xp < hi && fw > sm.thi[t]) {
+    if (xp > lo && xp < hi && (long long)s != sm.nflip[t]) {
         // Only the countdown ran out: a frame and/or the last step.
         const float F = sm.F[t];
         const float vk = OVER ? 0.0f : fmaf(F, sm.c1[t], rv);
@@ -520,7 +528,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
             sm.fidx[t] += 1;
             sm.nxf[t] += (long long)J.freq_save;
         }
-        sm.left[t] = steps_to_special(J, s, sm.nxf[t]);
+        sm.left[t] = steps_to_special(J, s, sm.nxf[t], sm.nflip[t]);
         if (s == J.nsteps) retire(s, vk, 0);
         return;
     }
@@ -549,23 +557,20 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     const bool dCell = cell != cell_prev;
     const bool dWell = well != well_prev;
     const bool dKey = DBL ? (lb != lb_prev) : dCell;
-    uint32_t thi = sm.thi[t];
-    int st = state;
-    if (fw <= thi) {
-        bool flip = fw < thi;
-        if (fw == thi) {
-            const uint64_t T = J.eq ? J.T_eq : J.T_as[st];
-            flip = philox_at(s, traj, TAG_REFINE, J.key0, J.key1).w0 < (uint32_t)T;
-        }
-        st ^= (int)flip;
-    }
+    // the current barrier flips at its scheduled step; a flip or a barrier
+    // change schedules the next one
+    const bool flip = (long long)s == sm.nflip[t];
+    int st = state ^ (int)flip;
     if (dKey) st = enter(fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb));
     if (DBL) sw = (sw & ~W_LB) | (lb ? W_LB : 0);
     if (st != state) {
         if (st) sm.since[t] = (long long)s;
         else sm.sc1[t] += (long long)s - sm.since[t];
         state = st;
-        thi = thi_of(J, st);
+    }
+    if (J.eta && (flip || dKey)) {
+        sm.nflip[t] = next_flip(J, traj, s, state);
+        left = 0;   // recompute the countdown below
     }
     band_of<DBL>(J, xp, &lo, &hi);
     const float F = force_of<DBL>(J, xp, state);
@@ -579,7 +584,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
             sm.nxf[t] += (long long)J.freq_save;
         }
         if (s == J.nsteps) finish = true;
-        left = steps_to_special(J, s, sm.nxf[t]);
+        left = steps_to_special(J, s, sm.nxf[t], sm.nflip[t]);
     }
     sm.xp[t] = xp;
     sm.cell[t] = cell;
@@ -587,7 +592,6 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     sm.sw[t] = sw;
     sm.lo[t] = lo;
     sm.hi[t] = hi;
-    sm.thi[t] = thi;
     sm.F[t] = F;
     sm.left[t] = left;
     if (finish) retire(s, vk, 0);
@@ -604,7 +608,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
 
 template <bool DBL, bool OVER>
 __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kernel(
-    const __grid_constant__ QueueDev q, const __grid_constant__ SlotsDev S, uint32_t pair_budget) {
+    const __grid_constant__ QueueDev q, const __grid_constant__ SlotsDev S, uint32_t quad_budget) {
     __shared__ RareSm sm;
     const int t = threadIdx.x;
     const int64_t slot = (int64_t)blockIdx.x * blockDim.x + t;
@@ -614,9 +618,8 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
     // ---- hot lane state (registers); the rest lives in sm ----
     int job = (slot < S.nslots) ? S.job[slot] : -1;
     uint32_t traj = 0;
-    uint64_t j = 0;                 // next pair: steps 2j+1, 2j+2
+    uint64_t j = 0;                 // next block of four steps: 4j+1 .. 4j+4
     float xp = 0.f, rv = 0.f, F = 0.f, lo = -kInf, hi = kInf;
-    uint32_t thi = 0;
     int left = kLeftMax;
     float c1 = 0.f, c2 = 0.f, c3 = 0.f, kn = 0.f;
     uint32_t key0 = 0, key1 = 0;
@@ -634,11 +637,10 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         key0 = J.key0;
         key1 = J.key1;
         const int state = sm.state[t];
-        thi = thi_of(J, state);
         band_of<DBL>(J, xp, &lo, &hi);
         F = force_of<DBL>(J, xp, state);
-        left = steps_to_special(J, s - 1, sm.nxf[t]);
-        j = (s - 1) >> 1;
+        left = steps_to_special(J, s - 1, sm.nxf[t], sm.nflip[t]);
+        j = (s - 1) >> 2;
     };
 
     if (job >= 0) {
@@ -666,11 +668,12 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         sm.cgw[t] = S.cgw[slot];
         sm.fidx[t] = S.fidx[slot];
         sm.nxf[t] = S.nxf[slot];
+        sm.nflip[t] = S.nflip[slot];
         bind(s);
     }
 
     bool dry = false;   // the queue had nothing left for this warp
-    for (uint32_t it = 0; it < pair_budget; ++it) {
+    for (uint32_t it = 0; it < quad_budget; ++it) {
         // ---- warp-aggregated refill of idle lanes ----
         const unsigned idle = __ballot_sync(kFull, job < 0);
         if (__builtin_expect(idle != 0, 0)) {
@@ -713,7 +716,6 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
                             sm.job[t] = -1;
                             lo = -kInf;
                             hi = kInf;
-                            thi = 0;
                             F = 0.f;
                             left = kLeftMax;
                         }
@@ -727,14 +729,14 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
             if (job < 0) continue;
         }
 
-        // ---- one Philox block, two steps ----
+        // ---- one Philox block, four steps ----
         const Words w = philox_wide((uint32_t)j, (uint32_t)(j >> 32), traj, TAG_STEP, key0, key1);
-        float n0, n1;
-        noise_pair(w.w0, w.w1, kn, &n0, &n1);
+        float nq[4];
+        noise_pair(w.w0, w.w1, kn, &nq[0], &nq[1]);
+        noise_pair(w.w2, w.w3, kn, &nq[2], &nq[3]);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const float nz = h ? n1 : n0;
-            const uint32_t fw = h ? w.w3 : w.w2;
+        for (int h = 0; h < 4; ++h) {
+            const float nz = nq[h];
             if (OVER) {
                 xp = fmaf(F, c1, xp);
                 xp = xp + nz;
@@ -747,20 +749,18 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
                 xp = fmaf(rv, c2, xp);
             }
             --left;
-            if (__builtin_expect(!(xp > lo && xp < hi) || fw <= thi || left == 0, 0)) {
+            if (__builtin_expect(!(xp > lo && xp < hi) || left == 0, 0)) {
                 sm.xp[t] = xp;
                 sm.rv[t] = rv;
                 sm.F[t] = F;
                 sm.left[t] = left;
                 sm.lo[t] = lo;
                 sm.hi[t] = hi;
-                sm.thi[t] = thi;
-                general_step<DBL, OVER>(q.jobs, &S, &sm, t, slot, 2 * j + 1 + h, fw);
+                general_step<DBL, OVER>(q.jobs, &S, &sm, t, slot, 4 * j + 1 + h);
                 xp = sm.xp[t];
                 F = sm.F[t];
                 lo = sm.lo[t];
                 hi = sm.hi[t];
-                thi = sm.thi[t];
                 left = sm.left[t];
                 job = sm.job[t];
             }
@@ -774,7 +774,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
     if (job >= 0) {
         const JobF& J = q.jobs[job];
         S.traj[slot] = traj;
-        S.step[slot] = (int64_t)(2 * j + 1);
+        S.step[slot] = (int64_t)(4 * j + 1);
         S.xp[slot] = xp;
         S.rv[slot] = rv;
         S.cell[slot] = sm.cell[t];
@@ -786,6 +786,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         S.cgw[slot] = sm.cgw[t];
         S.fidx[slot] = sm.fidx[t];
         S.nxf[slot] = sm.nxf[t];
+        S.nflip[slot] = sm.nflip[t];
         J.bits[traj] = (int32_t)sm.bits[t];
         J.init_idx0[traj] = sm.init0[t];
         J.idx2_0[traj] = sm.idx2[t];
@@ -836,13 +837,14 @@ int fp32_blocks_per_sm(bool dbl, bool over, int block) {
 int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint32_t pair_budget, int grid,
                            int block, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t quad_budget = pair_budget > 1 ? pair_budget / 2 : 1;   // blocks of four steps
     if (block > kMaxBlock) return (int)cudaErrorInvalidValue;
     if (dbl) {
-        if (over) fp32_persistent_kernel<true, true><<<grid, block, 0, st>>>(q, s, pair_budget);
-        else fp32_persistent_kernel<true, false><<<grid, block, 0, st>>>(q, s, pair_budget);
+        if (over) fp32_persistent_kernel<true, true><<<grid, block, 0, st>>>(q, s, quad_budget);
+        else fp32_persistent_kernel<true, false><<<grid, block, 0, st>>>(q, s, quad_budget);
     } else {
-        if (over) fp32_persistent_kernel<false, true><<<grid, block, 0, st>>>(q, s, pair_budget);
-        else fp32_persistent_kernel<false, false><<<grid, block, 0, st>>>(q, s, pair_budget);
+        if (over) fp32_persistent_kernel<false, true><<<grid, block, 0, st>>>(q, s, quad_budget);
+        else fp32_persistent_kernel<false, false><<<grid, block, 0, st>>>(q, s, quad_budget);
     }
     return (int)cudaGetLastError();
 }

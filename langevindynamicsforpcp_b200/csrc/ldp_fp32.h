@@ -49,6 +49,7 @@ struct JobF {
     double x0, v0, dt, Ld, invL, sig_v0, sig_r_d, a_lap, c_lap[2], p_first, p_cell0, mhalf;
     double Hs[2], Hd[2][2], iN[2][2], iP[2][2], sNd[2][2], sPd[2][2], wd, xbd[2], lo0d, hi1d, xcd;
     uint64_t T_eq, T_as[2];
+    double ln1m[2];      // log(1 - per-step flip probability) by state; 0: never flips
     uint64_t nsteps, freq_save;
     int64_t nframe, tick_cap, ntraj;
     // per-trajectory outputs [field][ntraj] (job local)
@@ -93,6 +94,7 @@ struct SlotsDev {
     int64_t *sc1, *since;   // completed state-1 steps; start of the current state-1 run
     int32_t *cgw, *fidx;    // well of the last FPTCG evaluation; index of the next frame
     int64_t* nxf;           // step of the next frame
+    int64_t* nflip;         // step of the current barrier's next flip
     longlong2* ring;        // [R][nslots] cell table: {key, stamp << 1 | state}
     unsigned long long* retired;   // total retired trajectories (all jobs)
     int32_t ring_slots;

@@ -91,7 +91,7 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     Q.rem = (unsigned long long*)(a + o);
     // slots
     const int R = ring_slots;
-    size_t sb = al256(sizeof(int32_t) * nslots) * 6 + al256(sizeof(int64_t) * nslots) * 6 +
+    size_t sb = al256(sizeof(int32_t) * nslots) * 6 + al256(sizeof(int64_t) * nslots) * 7 +
                 al256(sizeof(float) * nslots) * 2 + al256(sizeof(longlong2) * (size_t)R * nslots) +
                 al256(sizeof(unsigned long long));
     e = cudaMalloc(&Q.smem, sb);
@@ -109,6 +109,7 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     S.cgw = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
     S.fidx = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
     S.nxf = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.nflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.traj = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.step = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.cstamp = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
@@ -190,6 +191,7 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
     J->Hs[0] = k.Hs[0]; J->Hs[1] = k.Hs[1]; J->wd = k.w;
     J->xbd[0] = k.xb[0]; J->xbd[1] = k.xb[1]; J->lo0d = k.lo0; J->hi1d = k.hi1; J->xcd = k.xc;
     J->T_eq = k.T_eq; J->T_as[0] = k.T_as[0]; J->T_as[1] = k.T_as[1];
+    J->ln1m[0] = k.ln1m[0]; J->ln1m[1] = k.ln1m[1];
     J->nsteps = job->nsteps;
     J->freq_save = k.freq_save;
     J->nframe = k.nframe;

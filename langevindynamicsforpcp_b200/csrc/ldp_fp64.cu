@@ -221,6 +221,12 @@ __global__ void __launch_bounds__(128) fp64_init_kernel(const KConst k, const Tr
     gauss_pair_f64(w0.w1, w0.w2, &zv, &zr);
     t.v = k.rv ? k.sig_v0 * zv : k.v0;
     st.v0[i] = t.v;
+    {
+        // waiting time to the initial barrier's first flip
+        const Words wf = philox_at(0, g, TAG_FLIP, k.key0, k.key1);
+        const uint64_t wt = flip_wait(wf.w0, wf.w1, k.ln1m[t.state]);
+        st.nflip[i] = (int64_t)(wt == 0xffffffffffffffffull ? 0x7fffffffffffffffull : wt);
+    }
     energy_force<DBL>(k, t);
     if (k.at_bottom) {
         if (!DBL && k.fpt) fpt_set_initial<DBL>(k, st, i, g, t);
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(128) fp64_init_kernel(const KConst k, const Tr
 // IntegrateStepEta / IntegrateStep (S.h:1654-1706, 2833-2886; D.h:1973-2024,
 // 3448-3505) followed by UpdateStatistics (S.h:2334-2592, D.h:2931-3209).
 template <bool DBL, bool OVER, bool ETA>
-__global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const TrajState st, int64_t g0,
+__global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, const TrajState st, int64_t g0,
                                                          uint64_t s_begin, uint64_t s_end) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.n) return;
@@ -257,17 +263,26 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
     int64_t sc1 = st.counts[(int64_t)LDP_C_STATE1 * n + i];
     // Force at the current position (not stored between launches).
     energy_force<DBL>(k, t);
+    int64_t nflip = st.nflip[i];
     uint32_t flags = 0;
     uint64_t s = s_begin;
     const uint64_t fs = k.freq_save;
+    // One Philox block serves steps 4a+1 .. 4a+4: words 0,1 the first
+    // Gaussian pair, words 2,3 (kept) the second.
+    double za = 0, zb = 0;
+    uint32_t wc2 = 0, wc3 = 0;
     for (; s < s_end; ++s) {
-        const uint64_t j = (s - 1) >> 1;
-        const bool odd = ((s - 1) & 1) != 0;
-        const Words w = philox_at(j, g, TAG_STEP, k.key0, k.key1);
-        double za, zb;
-        gauss_pair_f64(w.w0, w.w1, &za, &zb);
-        const double z = odd ? zb : za;
-        const uint32_t fw = odd ? w.w3 : w.w2;
+        const int q = (int)((s - 1) & 3);
+        if (q == 0 || s == s_begin) {
+            const Words w = philox_at((s - 1) >> 2, g, TAG_STEP, k.key0, k.key1);
+            wc2 = w.w2;
+            wc3 = w.w3;
+            if (q < 2) gauss_pair_f64(w.w0, w.w1, &za, &zb);
+            else gauss_pair_f64(w.w2, w.w3, &za, &zb);
+        } else if (q == 2) {
+            gauss_pair_f64(wc2, wc3, &za, &zb);
+        }
+        const double z = (q & 1) ? zb : za;
 
         const int64_t cell_prev = t.cell, well_prev = t.well;
         const int lb_prev = t.lb;
@@ -294,14 +309,11 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
         const bool dKey = DBL ? (t.lb != lb_prev) : dCell;
 
         if (ETA) {
-            // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736.
-            const uint64_t T = k.eq ? k.T_eq : k.T_as[t.state];
-            const uint32_t Thi = (uint32_t)(T >> 32), Tlo = (uint32_t)T;
-            bool flip = fw < Thi;
-            if (fw == Thi) {
-                const Words wr = philox_at(s, g, TAG_REFINE, k.key0, k.key1);
-                flip = wr.w0 < Tlo;
-            }
+            // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736: the
+            // current barrier flips at its scheduled step (geometric waiting
+            // times of the per-step Bernoulli flips); a flip or a barrier
+            // change schedules the next flip.
+            const bool flip = (int64_t)s == nflip;
             if (flip) t.state ^= 1;
             if (dKey) {
                 ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, (int64_t)s);
@@ -314,6 +326,11 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
                 const Words wc = philox_at(s, g, TAG_CATCHUP, k.key0, k.key1);
                 const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
                 t.state = (U < Tl) ? (ps ^ 1) : ps;
+            }
+            if (flip || dKey) {
+                const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+                const uint64_t wt = flip_wait(wf.w0, wf.w1, k.ln1m[t.state]);
+                nflip = (wt >= 0x7fffffffffffffffull - s) ? 0x7fffffffffffffffll : (int64_t)(s + wt);
             }
         } else {
             // UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434.
@@ -420,6 +437,7 @@ __global__ void __launch_bounds__(128) fp64_steps_kernel(const KConst k, const T
     st.counts[(int64_t)LDP_C_STEPS * n + i] = (int64_t)s - 1;
     if (k.fp_mode && !(t.bits & B_DONE) && s_end > k.step_cap) flags |= LDP_FLAG_CENSORED;
     if (flags) st.counts[(int64_t)LDP_C_FLAGS * n + i] |= (int64_t)flags;
+    st.nflip[i] = nflip;
     store_traj(st, t, i);
 }
 

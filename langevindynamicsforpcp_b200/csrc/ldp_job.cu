@@ -280,7 +280,7 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o0 = off; off += align256(bytes); return o0; };
     const size_t o_d = take(sizeof(double) * 9 * n);
-    const size_t o_i64 = take(sizeof(int64_t) * 8 * n);
+    const size_t o_i64 = take(sizeof(int64_t) * 9 * n);
     const size_t o_i32 = take(sizeof(int32_t) * 4 * n);
     const size_t o_cg = take(sizeof(double) * ncg_rows * n);
     const size_t o_cgw = take(sizeof(int64_t) * ncg_rows * n);
@@ -314,7 +314,7 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     S.fpt2_last = dd + 5 * n; S.tpt_last = dd + 6 * n; S.tpt2_last = dd + 7 * n; S.v0 = dd + 8 * n;
     int64_t* ii = (int64_t*)(a + o_i64);
     S.cell = ii; S.well = ii + n; S.init_idx0 = ii + 2 * n; S.init_idx1 = ii + 3 * n; S.idx2_0 = ii + 4 * n;
-    S.idx2_1 = ii + 5 * n; S.tpt2_well = ii + 6 * n; S.wt_tick = ii + 7 * n;
+    S.idx2_1 = ii + 5 * n; S.tpt2_well = ii + 6 * n; S.wt_tick = ii + 7 * n; S.nflip = ii + 8 * n;
     int32_t* i32 = (int32_t*)(a + o_i32);
     S.state = i32; S.lb = i32 + n; S.bits = i32 + 2 * n; S.state0 = i32 + 3 * n;
     S.cg_last = (double*)(a + o_cg);

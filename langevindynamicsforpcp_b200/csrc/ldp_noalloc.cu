@@ -24,7 +24,7 @@
 namespace {
 
 constexpr int kSlots = 64;                       // cell-table ring slots per trajectory
-constexpr int64_t kPerTraj = 9 * 8 + 8 * 8 + 4 * 4 + 2 * LDP_MAX_CG * 8 + 2 * kSlots * 8;
+constexpr int64_t kPerTraj = 9 * 8 + 9 * 8 + 4 * 4 + 2 * LDP_MAX_CG * 8 + 2 * kSlots * 8;
 constexpr size_t kLdpNoallocScratchBytes = (size_t)LDP_NOALLOC_MAX_TRAJ * kPerTraj + 64 * 256;
 
 // The working state shared by every call on a device.
@@ -104,9 +104,9 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
     double* dd = (double*)take(sizeof(double) * 9 * n);
     S.x = d_x_final; S.v = dd + n; S.F = dd + 2 * n; S.rprev = dd + 3 * n; S.fpt_last = dd + 4 * n;
     S.fpt2_last = dd + 5 * n; S.tpt_last = dd + 6 * n; S.tpt2_last = dd + 7 * n; S.v0 = dd + 8 * n;
-    int64_t* ii = (int64_t*)take(sizeof(int64_t) * 8 * n);
+    int64_t* ii = (int64_t*)take(sizeof(int64_t) * 9 * n);
     S.cell = ii; S.well = ii + n; S.init_idx0 = ii + 2 * n; S.init_idx1 = ii + 3 * n; S.idx2_0 = ii + 4 * n;
-    S.idx2_1 = ii + 5 * n; S.tpt2_well = ii + 6 * n; S.wt_tick = ii + 7 * n;
+    S.idx2_1 = ii + 5 * n; S.tpt2_well = ii + 6 * n; S.wt_tick = ii + 7 * n; S.nflip = ii + 8 * n;
     int32_t* i32 = (int32_t*)take(sizeof(int32_t) * 4 * n);
     S.state = i32; S.lb = i32 + n; S.bits = i32 + 2 * n; S.state0 = i32 + 3 * n;
     S.cg_last = (double*)take(sizeof(double) * LDP_MAX_CG * n);

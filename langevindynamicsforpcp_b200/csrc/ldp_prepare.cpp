@@ -125,6 +125,12 @@ void prepare_kconst(const ldp_params& p, const ldp_job_opts& o, uint32_t seed, K
         k->c_lap[1] = 1.0 / (1.0 + K);
         k->p_first = 1.0 / (1.0 + K);
     }
+    // Waiting times between flips (geometric in the per-step probability).
+    for (int s = 0; s < 2; ++s) {
+        double pf = 0.0;
+        if (k->eta) pf = k->eq ? 0.5 * -std::expm1(-2.0 * k->dt / p.tau) : k->c_lap[s] * -std::expm1(k->a_lap);
+        k->ln1m[s] = (pf > 0.0) ? std::log1p(-pf) : 0.0;
+    }
     k->p_cell0 = 1.0 / (1.0 + K);   // BarrierStatus::Initialize, S.h:90
     // Math::Modulo(X0, L) == L/2 (S.h:2184, src/mathdef.h:20).
     k->at_bottom = std::fmod(std::fmod(k->x0, k->L) + k->L, k->L) == halfL;

@@ -22,7 +22,7 @@
 #define TAG_INIT 1u
 #define TAG_CATCHUP 2u
 #define TAG_CELL 3u
-#define TAG_REFINE 4u
+#define TAG_FLIP 4u
 
 /* ---------------------------------------------------------------------- */
 /* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11, "Parallel random
@@ -149,6 +149,18 @@ double ldpo_expm1(double x) {
     return fma(s, e, s - 1.0);
 }
 
+/* Steps to the next flip of a barrier flipping with probability p per step
+ * (ln1m = log(1 - p)): W = 1 + floor(ln U / ln(1 - p)), U in (0, 1] from the
+ * 64-bit word pair -- the geometric waiting time of the reference's per-step
+ * Bernoulli flips (S.h:2010-2015); UINT64_MAX when the barrier never flips. */
+uint64_t ldpo_flip_wait(uint32_t hi, uint32_t lo, double ln1m) {
+    if (!(ln1m < 0.0)) return UINT64_MAX;
+    const double u = ((double)(((uint64_t)hi << 32) | lo) + 1.0) * 0x1p-64;
+    const double q = ldpo_log(u) / ln1m;
+    if (!(q < 0x1p62)) return UINT64_MAX;
+    return 1ull + (uint64_t)floor(q);
+}
+
 uint64_t ldpo_prob_to_u64(double p) {
     if (!(p > 0.0)) return 0;
     if (p >= 1.0) return UINT64_MAX;
@@ -178,6 +190,7 @@ typedef struct {
     double xb[2], lo0, hi1, xc, Hd[2][2], sN[2][2], sP[2][2], iN[2][2], iP[2][2];
     double c_drift, sig_r, invM, hdt, expg, sig_v, mhalf, sig_v0;
     uint64_t T_eq, T_as[2];
+    double ln1m[2];    /* log(1 - per-step flip probability) by state; 0: never */
     double a_lap, c_lap[2];
     double p_first, p_cell0;
     int at_bottom;
@@ -281,6 +294,12 @@ static void prepare(const ldp_params *p, ocst *k) {
         k->c_lap[0] = K / (1.0 + K);
         k->c_lap[1] = 1.0 / (1.0 + K);
         k->p_first = 1.0 / (1.0 + K);
+    }
+    /* Waiting times between flips: geometric in the per-step probability. */
+    for (int s = 0; s < 2; ++s) {
+        double pf = 0.0;
+        if (k->eta) pf = k->eq ? 0.5 * -expm1(-2.0 * k->dt / p->tau) : k->c_lap[s] * -expm1(k->a_lap);
+        k->ln1m[s] = (pf > 0.0) ? log1p(-pf) : 0.0;
     }
     k->p_cell0 = 1.0 / (1.0 + K);   /* BarrierStatus::Initialize, S.h:90 */
     /* Math::Modulo(X0, L) == L/2, S.h:2184, src/mathdef.h:20 */
@@ -524,6 +543,13 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
         gauss_pair(w0[1], w0[2], &zv, &zr);
         t.v = k->rv ? k->sig_v0 * zv : k->v0;
         double v0inst = t.v;
+        int64_t nflip;
+        {
+            uint32_t wf[4];
+            philox_at(0, g, TAG_FLIP, key, wf);
+            const uint64_t wt = ldpo_flip_wait(wf[0], wf[1], k->ln1m[t.state]);
+            nflip = (wt == UINT64_MAX) ? INT64_MAX : (int64_t)wt;
+        }
         energy_force(k, &t);
         /* InitializeStatistics, S.h:2166-2333 */
         t.wt_tick = 0;
@@ -559,15 +585,17 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
         uint64_t s;
         uint64_t done_steps = 0;
         int stop = 0;
+        double zq[4];
         for (s = 1; s <= nsteps && !stop; ++s) {
-            const uint64_t j = (s - 1) >> 1;
-            const int odd = (int)((s - 1) & 1);
-            uint32_t w[4];
-            philox_at(j, g, TAG_STEP, key, w);
-            double za, zb;
-            gauss_pair(w[0], w[1], &za, &zb);
-            const double z = odd ? zb : za;
-            const uint32_t fw = odd ? w[3] : w[2];
+            /* one Philox block: the Gaussians of steps 4a+1 .. 4a+4 */
+            const int qi = (int)((s - 1) & 3);
+            if (qi == 0) {
+                uint32_t w[4];
+                philox_at((s - 1) >> 2, g, TAG_STEP, key, w);
+                gauss_pair(w[0], w[1], &zq[0], &zq[1]);
+                gauss_pair(w[2], w[3], &zq[2], &zq[3]);
+            }
+            const double z = zq[qi];
 
             const int64_t cell_prev = t.cell, well_prev = t.well;
             const int lb_prev = t.lb;
@@ -592,15 +620,10 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
             const int dKey = k->dbl ? (t.lb != lb_prev) : dCell;
 
             if (k->eta) {
-                /* UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736 */
-                uint64_t T = k->eq ? k->T_eq : k->T_as[t.state];
-                uint32_t Thi = (uint32_t)(T >> 32), Tlo = (uint32_t)T;
-                int flip = fw < Thi;
-                if (fw == Thi) {
-                    uint32_t wr[4];
-                    philox_at(s, g, TAG_REFINE, key, wr);
-                    flip = wr[0] < Tlo;
-                }
+                /* UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736: the
+                 * current barrier flips at its scheduled step; a flip or a
+                 * barrier change schedules the next one (below). */
+                const int flip = (int64_t)s == nflip;
                 if (flip) t.state ^= 1;
                 if (dKey) {
                     ring_store(&r, cell_key(k, cell_prev, lb_prev), t.state, (int64_t)s, &evict);
@@ -614,6 +637,12 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                     philox_at(s, g, TAG_CATCHUP, key, wc);
                     uint64_t U = ((uint64_t)wc[0] << 32) | wc[1];
                     t.state = (U < Tl) ? (ps ^ 1) : ps;
+                }
+                if (flip || dKey) {
+                    uint32_t wf[4];
+                    philox_at(s, g, TAG_FLIP, key, wf);
+                    const uint64_t wt = ldpo_flip_wait(wf[0], wf[1], k->ln1m[t.state]);
+                    nflip = (wt >= (uint64_t)INT64_MAX - s) ? INT64_MAX : (int64_t)(s + wt);
                 }
             } else {
                 /* UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434 */

@@ -34,6 +34,7 @@ double   ldpo_log(double u);
 void     ldpo_sincos2pi(double t, double *s, double *c);
 double   ldpo_expm1(double x);
 uint64_t ldpo_prob_to_u64(double p);
+uint64_t ldpo_flip_wait(uint32_t hi, uint32_t lo, double ln1m);
 
 /* Steps integrated per trajectory and frames recorded, as the reference's
  * Integrate loop does them (S.h:1403-1511). */
