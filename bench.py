@@ -37,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 OPS_PER_STEP = 70   # lane instructions per overdamped single-barrier step (algorithmic count)
+# Source-level count of the FP32 hot loop as built: a Philox block (58) per
+# four steps, two Box-Muller pairs (14 each), update 3, tests 3.
+OPS_PER_STEP_AS_BUILT = (58 + 2 * 14) / 4 + 3 + 3
 NJOBS, NTRAJ, NSTEPS, FREQSAVE = 16, 65536, 300000, 100
 # DRAM bytes per particle-step of the persistent kernel: 0.434 B measured by
 # ncu with frames every 20 steps (8 B per frame = 0.40 B per step of it);
@@ -342,6 +345,8 @@ def main():
                                  "scaled by particle-steps and frame interval; algorithmic bytes: the frames, 8 B per FREQSAVE steps",
                 "kernel": "fp32_persistent_kernel<single, overdamped>",
                 "ops_per_step": OPS_PER_STEP, "kernel_ms": kms,
+                "ops_per_step_as_built": OPS_PER_STEP_AS_BUILT,
+                "frac_as_built": psteps * OPS_PER_STEP_AS_BUILT / (kms * 1e-3) / 1e9 / peak_issue,
                 "peak_basis": f"{sms} SMs x 128 lanes x sm_max_mhz {fmax:g} (MEASURED_PEAKS.json)",
                 "frac_at_sampled_clock": achieved / (sms * 128 * fclk * 1e6 / 1e9)}
 

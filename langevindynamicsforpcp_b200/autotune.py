@@ -30,7 +30,7 @@ MODELS = {"single_over": (False, True), "single_under": (False, False),
 CANDIDATES = [(block, bps, pb) for block in (128, 256) for bps in (0,) for pb in (4096, 16384, 65536)]
 
 
-def workload(model: str, steps: int, njobs: int, ntraj: int):
+def workload(model: str, steps: int, njobs: int, ntraj: int, freqsave: int = 100):
     """njobs jobs of the model: CuIDB geometry, H_low in {2, 3, 4, 5},
     flip rate logU[1e-2, 1e2], gamma 1, drawn with default_rng(1234)."""
     dbl, over = MODELS[model]
@@ -39,7 +39,7 @@ def workload(model: str, steps: int, njobs: int, ntraj: int):
     for _ in range(njobs):
         h = float(rng.choice([2.0, 3.0, 4.0, 5.0]))
         k = float(10 ** rng.uniform(-2, 2))
-        text = COMMON.format(over="true" if over else "false", gamma=1.0, steps=steps, freq=20, tau=1.0 / k,
+        text = COMMON.format(over="true" if over else "false", gamma=1.0, steps=steps, freq=freqsave, tau=1.0 / k,
                              seed=1234)
         text += DOUBLE.format(mid=1.7 * h, high=3.6 * h, low=h) if dbl else SINGLE.format(high=3.6 * h, low=h)
         out.append(params_from_inp_text(text, MODEL_DOUBLE if dbl else MODEL_SINGLE))
@@ -70,7 +70,8 @@ def main(argv=None):
     here = os.path.dirname(os.path.abspath(__file__))
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(here, "tuning.json"))
-    ap.add_argument("--steps", type=int, default=24000)
+    ap.add_argument("--steps", type=int, default=120000)
+    ap.add_argument("--freqsave", type=int, default=100)
     ap.add_argument("--jobs", type=int, default=4)
     ap.add_argument("--ntraj", type=int, default=65536)
     ap.add_argument("--repeat", type=int, default=2)
@@ -83,7 +84,7 @@ def main(argv=None):
                           f"(CuIDB geometry, H_low in {{2,3,4,5}}, flip rate logU[1e-2,1e2])",
               "trajectories_per_thread": 1, "shapes": {}, "trials": []}
     for model in a.models:
-        params, ntraj = workload(model, a.steps, a.jobs, a.ntraj)
+        params, ntraj = workload(model, a.steps, a.jobs, a.ntraj, a.freqsave)
         psteps = a.jobs * ntraj * a.steps
         best = None
         for shape in CANDIDATES:

@@ -16,14 +16,17 @@
 //   TAG_CELL    a = cell key: word 0 -> state of a never-visited cell
 //               (BarrierStatus::Initialize, S.h:78-96).
 //   TAG_FLIP    a = step: words 0,1 -> 64-bit uniform of the waiting time to
-//               the current barrier's next flip, drawn at step 0 and at every
-//               step whose barrier state or barrier changed.
+//               the current barrier's next flip, drawn at step 0, after every
+//               flip, and on a barrier change that changes the flip
+//               probability.
 //
 // The reference flips the current barrier with probability p each step
 // (S.h:2010-2015); those flips form a Bernoulli process, so the steps
 // between them are geometric, and drawing the waiting time once per flip
-// (or per barrier change: the process is memoryless) gives the same process
-// while each step needs only its Gaussian.
+// gives the same process while each step needs only its Gaussian.  The
+// process is memoryless: across a change of barrier with the same flip
+// probability the pending waiting time stays valid, with a different one a
+// new one is drawn.
 //
 // The FP64 functions below evaluate a fixed operation sequence with explicit
 // fma() so that the FP64 device path is bit-identical to a host evaluation

@@ -561,6 +561,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     // change schedules the next one
     const bool flip = (long long)s == sm.nflip[t];
     int st = state ^ (int)flip;
+    const int st_flip = st;
     if (dKey) st = enter(fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb));
     if (DBL) sw = (sw & ~W_LB) | (lb ? W_LB : 0);
     if (st != state) {
@@ -568,7 +569,9 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
         else sm.sc1[t] += (long long)s - sm.since[t];
         state = st;
     }
-    if (J.eta && (flip || dKey)) {
+    // a pending waiting time stays valid across a barrier change whose flip
+    // probability is the same (memoryless)
+    if (J.eta && (flip || (dKey && J.ln1m[st] != J.ln1m[st_flip]))) {
         sm.nflip[t] = next_flip(J, traj, s, state);
         left = 0;   // recompute the countdown below
     }

@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
             // change schedules the next flip.
             const bool flip = (int64_t)s == nflip;
             if (flip) t.state ^= 1;
+            const int st_flip = t.state;
             if (dKey) {
                 ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, (int64_t)s);
                 int ps;
@@ -327,7 +328,9 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
                 const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
                 t.state = (U < Tl) ? (ps ^ 1) : ps;
             }
-            if (flip || dKey) {
+            // A pending waiting time stays valid across a barrier change
+            // whose flip probability is the same (memoryless).
+            if (flip || (dKey && k.ln1m[t.state] != k.ln1m[st_flip])) {
                 const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
                 const uint64_t wt = flip_wait(wf.w0, wf.w1, k.ln1m[t.state]);
                 nflip = (wt >= 0x7fffffffffffffffull - s) ? 0x7fffffffffffffffll : (int64_t)(s + wt);

@@ -625,6 +625,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                  * barrier change schedules the next one (below). */
                 const int flip = (int64_t)s == nflip;
                 if (flip) t.state ^= 1;
+                const int st_flip = t.state;
                 if (dKey) {
                     ring_store(&r, cell_key(k, cell_prev, lb_prev), t.state, (int64_t)s, &evict);
                     int ps;
@@ -638,7 +639,9 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                     uint64_t U = ((uint64_t)wc[0] << 32) | wc[1];
                     t.state = (U < Tl) ? (ps ^ 1) : ps;
                 }
-                if (flip || dKey) {
+                /* A pending waiting time stays valid across a barrier change
+                 * whose flip probability is the same (memoryless). */
+                if (flip || (dKey && k->ln1m[t.state] != k->ln1m[st_flip])) {
                     uint32_t wf[4];
                     philox_at(s, g, TAG_FLIP, key, wf);
                     const uint64_t wt = ldpo_flip_wait(wf[0], wf[1], k->ln1m[t.state]);
