@@ -180,6 +180,15 @@ __device__ __forceinline__ uint64_t flip_wait(uint32_t hi, uint32_t lo, double l
     return 1ull + (uint64_t)floor(q);
 }
 
+// "Never" for a flip step; fits the cell table's (step << 1 | state).
+constexpr int64_t kNeverFlip = (int64_t)((1ull << 62) - 1);
+
+// Step of the next flip drawn at step s: s + W, clamped to kNeverFlip.
+__device__ __forceinline__ int64_t flip_schedule(uint64_t s, uint32_t hi, uint32_t lo, double ln1m) {
+    const uint64_t wt = flip_wait(hi, lo, ln1m);
+    return (wt >= (uint64_t)kNeverFlip - s) ? kNeverFlip : (int64_t)(s + wt);
+}
+
 __device__ __forceinline__ uint64_t prob_to_u64(double p) {
     if (!(p > 0.0)) return 0ull;
     if (p >= 1.0) return 0xffffffffffffffffull;

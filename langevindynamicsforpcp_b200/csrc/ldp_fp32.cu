@@ -64,7 +64,7 @@ struct RareSm {
     int32_t fidx[kMaxBlock];      // index of the next frame
     long long nxf[kMaxBlock];     // step of the next frame
     long long fpt[kMaxBlock], fpt2[kMaxBlock], tpt[kMaxBlock], tpt2[kMaxBlock];
-    long long cstamp[kMaxBlock];  // step at which the cached cell was left
+    long long cflip[kMaxBlock];   // pending flip step of the cached cell
     long long sc1[kMaxBlock];     // completed state-1 steps
     long long since[kMaxBlock];   // first step of the current state-1 run
     // Lane state the hot loop hands to the general step and takes back, and
@@ -82,12 +82,12 @@ __device__ __forceinline__ void red_add(int64_t* p, int64_t v) {
 __device__ __forceinline__ int fkey(bool dbl, int cell, int lb) { return dbl ? cell * 2 + lb : cell; }
 
 // Step of the next flip of a barrier now in state st, scheduled at step s
-// (words of TAG_FLIP at a = s; geometric waiting time, FP64 as in the FP64
-// path, so both precisions schedule the same flips from the same history).
+// (words w0:w1 of TAG_FLIP at a = s; geometric waiting time, FP64 as in the
+// FP64 path, so both precisions schedule the same flips from the same
+// history).
 __device__ __forceinline__ long long next_flip(const JobF& J, uint32_t traj, uint64_t s, int st) {
     const Words w = philox_at(s, traj, TAG_FLIP, J.key0, J.key1);
-    const uint64_t wt = flip_wait(w.w0, w.w1, J.ln1m[st]);
-    return (wt >= 0x7fffffffffffffffull - s) ? 0x7fffffffffffffffll : (long long)(s + wt);
+    return flip_schedule(s, w.w0, w.w1, J.ln1m[st]);
 }
 
 // Uniform in (0, 1): the high 23 bits of w as a mantissa, offset by 2^-24.
@@ -276,7 +276,7 @@ __device__ __noinline__ void f_start(const JobF* Jp, longlong2* ring, int64_t ns
     sm->nxf[t] = (!J.fp_mode && J.freq_save) ? (long long)J.freq_save : INT64_MAX;
     sm->nflip[t] = next_flip(J, traj, 0, st);
     sm->fpt[t] = sm->fpt2[t] = sm->tpt[t] = sm->tpt2[t] = 0;
-    sm->cstamp[t] = 0;
+    sm->cflip[t] = 0;
     sm->sc1[t] = 0;
     sm->since[t] = 0;
     *xp = (float)xpd;
@@ -376,43 +376,56 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
         sm.left[t] = kLeftMax;
     };
 
-    // Cell (double model: local barrier) entry: write the state of the key
-    // left through to the ring, take the entered key's state and stamp from
-    // the one-entry cache or the ring, and catch it up over the steps it was
-    // not observed (UpdateBarrierStateEta, S.h:2025-2068 / D.h:2468-2517).
-    auto enter = [&](int key_prev, int st, int key_cur) -> int {
+    // Cell (double model: local barrier) entry (UpdateBarrierStateEta,
+    // S.h:2025-2068 / D.h:2468-2517): write the state and pending flip step
+    // of the key left (*nf) through to the ring and the one-entry cache, take
+    // the entered key's from the cache or the ring.  A barrier re-entered
+    // before its pending flip has not flipped meanwhile; one whose flip came
+    // while it was away (or never visited: created at step 0) is caught up
+    // from that step and gets a new schedule (words w2:w3 of TAG_FLIP at s,
+    // *wf when the flip of this step already drew them).
+    auto enter = [&](int key_prev, int st, int key_cur, long long* nf, Words* wf, bool have_wf) -> int {
         const int64_t n = J.ntraj;
         const int rmask = S.ring_slots - 1;
         if (sw & W_EVICT) red_add(&J.counts[(int64_t)LDP_C_EVICT * n + traj], 1);
         S.ring[(int64_t)(key_prev & rmask) * S.nslots + slot] =
-            make_longlong2((long long)key_prev, (long long)((s << 1) | (uint64_t)st));
+            make_longlong2((long long)key_prev, (*nf << 1) | (long long)st);
         int ps;
-        int64_t stamp;
-        bool ev = false;
+        long long nb;
+        bool found = true, ev = false;
         if ((sw & W_CVALID) && sm.ckey[t] == key_cur) {
             ps = (sw & W_CSTATE) ? 1 : 0;
-            stamp = sm.cstamp[t];
+            nb = sm.cflip[t];
         } else {
             const longlong2 e = S.ring[(int64_t)(key_cur & rmask) * S.nslots + slot];
             if (e.x == (long long)key_cur) {
                 ps = (int)(e.y & 1);
-                stamp = e.y >> 1;
+                nb = e.y >> 1;
             } else {
                 ps = f_default_state(J, DBL, traj, key_cur);
-                stamp = 0;
+                nb = 0;
+                found = false;
                 ev = e.x != (long long)INT64_MIN;
             }
         }
         sm.ckey[t] = key_prev;
-        sm.cstamp[t] = (long long)s;
+        sm.cflip[t] = *nf;
         sw = (sw & W_LB) | W_CVALID | (st ? W_CSTATE : 0) | (ev ? W_EVICT : 0);
         if (!J.eta) return ps;
-        // Flip with probability c (1 - e^{a lap}), FP32, against the high
-        // word of the same catch-up uniform the FP64 path draws.
-        const float pl = J.c_lapf[J.eq ? 0 : ps] * one_minus_exp(J.a_lapf * (float)((int64_t)s - stamp));
+        if (found && nb > (long long)s) {
+            *nf = nb;
+            return ps;
+        }
+        // Flip with probability c (1 - e^{a lap}) over the steps since the
+        // missed flip, FP32, against the high word of the same catch-up
+        // uniform the FP64 path draws.
+        const int sb = found ? (ps ^ 1) : ps;
+        const float pl = J.c_lapf[J.eq ? 0 : sb] * one_minus_exp(J.a_lapf * (float)((long long)s - nb));
         const uint32_t w0 = philox_at(s, traj, TAG_CATCHUP, J.key0, J.key1).w0;
-        const bool flip = (pl >= 1.0f) || (w0 < (uint32_t)(pl * 4294967296.0f));
-        return flip ? (ps ^ 1) : ps;
+        const int sn = ((pl >= 1.0f) || (w0 < (uint32_t)(pl * 4294967296.0f))) ? (sb ^ 1) : sb;
+        if (!have_wf) *wf = philox_at(s, traj, TAG_FLIP, J.key0, J.key1);
+        *nf = flip_schedule(s, wf->w2, wf->w3, J.ln1m[sn]);
+        return sn;
     };
 
     // Renewal statistics (UpdateStatistics, S.h:2334-2592 / D.h:2931-3209)
@@ -557,22 +570,25 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     const bool dCell = cell != cell_prev;
     const bool dWell = well != well_prev;
     const bool dKey = DBL ? (lb != lb_prev) : dCell;
-    // the current barrier flips at its scheduled step; a flip or a barrier
-    // change schedules the next one
+    // the current barrier flips at its pending flip step and draws the next
+    // one; a barrier change takes the entered barrier's schedule
     const bool flip = (long long)s == sm.nflip[t];
     int st = state ^ (int)flip;
-    const int st_flip = st;
-    if (dKey) st = enter(fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb));
+    long long nf = sm.nflip[t];
+    Words wf{};
+    if (flip) {
+        wf = philox_at(s, traj, TAG_FLIP, J.key0, J.key1);
+        nf = flip_schedule(s, wf.w0, wf.w1, J.ln1m[st]);
+    }
+    if (dKey) st = enter(fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb), &nf, &wf, flip);
     if (DBL) sw = (sw & ~W_LB) | (lb ? W_LB : 0);
     if (st != state) {
         if (st) sm.since[t] = (long long)s;
         else sm.sc1[t] += (long long)s - sm.since[t];
         state = st;
     }
-    // a pending waiting time stays valid across a barrier change whose flip
-    // probability is the same (memoryless)
-    if (J.eta && (flip || (dKey && J.ln1m[st] != J.ln1m[st_flip]))) {
-        sm.nflip[t] = next_flip(J, traj, s, state);
+    if (J.eta && (flip || dKey)) {
+        sm.nflip[t] = nf;
         left = 0;   // recompute the countdown below
     }
     band_of<DBL>(J, xp, &lo, &hi);
@@ -665,7 +681,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         sm.tpt[t] = J.tpt_last[traj];
         sm.tpt2[t] = J.tpt2_last[traj];
         sm.ckey[t] = S.ckey[slot];
-        sm.cstamp[t] = S.cstamp[slot];
+        sm.cflip[t] = S.cflip[slot];
         sm.sc1[t] = S.sc1[slot];
         sm.since[t] = S.since[slot];
         sm.cgw[t] = S.cgw[slot];
@@ -783,7 +799,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         S.cell[slot] = sm.cell[t];
         S.st[slot] = sm.state[t] | (sm.sw[t] << 1);
         S.ckey[slot] = sm.ckey[t];
-        S.cstamp[slot] = sm.cstamp[t];
+        S.cflip[slot] = sm.cflip[t];
         S.sc1[slot] = sm.sc1[t];
         S.since[slot] = sm.since[t];
         S.cgw[slot] = sm.cgw[t];

@@ -90,7 +90,7 @@ struct SlotsDev {
     float *xp, *rv;         // rv: R_prev (overdamped) or v (underdamped)
     int32_t *cell, *st;     // st: state | slot flags << 1 (local barrier, cache, eviction)
     int32_t* ckey;          // key of the cell left last (cached state)
-    int64_t* cstamp;        // step at which it was left
+    int64_t* cflip;         // its pending flip step when it was left
     int64_t *sc1, *since;   // completed state-1 steps; start of the current state-1 run
     int32_t *cgw, *fidx;    // well of the last FPTCG evaluation; index of the next frame
     int64_t* nxf;           // step of the next frame

@@ -112,7 +112,7 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     S.nflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.traj = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.step = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.cstamp = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.cflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.sc1 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.since = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
     S.xp = (float*)(a + o); o += al256(sizeof(float) * nslots);

@@ -50,28 +50,33 @@ __device__ int default_state(const KConst& k, uint32_t g, int64_t ck) {
 }
 
 template <bool DBL>
+// A cell-table entry: the barrier's state when it was left and its pending
+// flip step; *found false for a cell never visited (state as drawn at its
+// creation, step 0).
 __device__ __forceinline__ void ring_load(const KConst& k, const TrajState& st, int64_t i, uint32_t g, int64_t ck,
-                                          int* state, int64_t* stamp) {
+                                          int* state, int64_t* nflip, bool* found) {
     const int64_t slot = ck & (int64_t)(k.slots - 1);
     const int64_t o = slot * st.n + i;
     if (st.ring_tag[o] == ck) {
         const int64_t d = st.ring_data[o];
         *state = (int)(d & 1);
-        *stamp = d >> 1;
+        *nflip = d >> 1;
+        *found = true;
     } else {
         *state = default_state<DBL>(k, g, ck);
-        *stamp = 0;
+        *nflip = 0;
+        *found = false;
     }
 }
 
 __device__ __forceinline__ void ring_store(const KConst& k, const TrajState& st, int64_t i, int64_t ck, int state,
-                                           int64_t stamp) {
+                                           int64_t nflip) {
     const int64_t slot = ck & (int64_t)(k.slots - 1);
     const int64_t o = slot * st.n + i;
     const int64_t old = st.ring_tag[o];
     if (old != ck && old != INT64_MIN) st.counts[(int64_t)LDP_C_EVICT * st.n + i] += 1;
     st.ring_tag[o] = ck;
-    st.ring_data[o] = (stamp << 1) | (int64_t)state;
+    st.ring_data[o] = (nflip << 1) | (int64_t)state;
 }
 
 // EnergyAndForce, S.h:1292-1324 / D.h:1464-1522.
@@ -125,8 +130,9 @@ template <bool DBL>
 __device__ __forceinline__ int table_state(const KConst& k, const TrajState& st, int64_t i, uint32_t g,
                                            int64_t cell) {
     int s;
-    int64_t stamp;
-    ring_load<DBL>(k, st, i, g, cell_key<DBL>(cell, 0), &s, &stamp);
+    int64_t nf;
+    bool found;
+    ring_load<DBL>(k, st, i, g, cell_key<DBL>(cell, 0), &s, &nf, &found);
     return s;
 }
 
@@ -224,8 +230,7 @@ __global__ void __launch_bounds__(128) fp64_init_kernel(const KConst k, const Tr
     {
         // waiting time to the initial barrier's first flip
         const Words wf = philox_at(0, g, TAG_FLIP, k.key0, k.key1);
-        const uint64_t wt = flip_wait(wf.w0, wf.w1, k.ln1m[t.state]);
-        st.nflip[i] = (int64_t)(wt == 0xffffffffffffffffull ? 0x7fffffffffffffffull : wt);
+        st.nflip[i] = flip_schedule(0, wf.w0, wf.w1, k.ln1m[t.state]);
     }
     energy_force<DBL>(k, t);
     if (k.at_bottom) {
@@ -309,39 +314,53 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
         const bool dKey = DBL ? (t.lb != lb_prev) : dCell;
 
         if (ETA) {
-            // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736: the
-            // current barrier flips at its scheduled step (geometric waiting
-            // times of the per-step Bernoulli flips); a flip or a barrier
-            // change schedules the next flip.
+            // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736, with
+            // every barrier's flips on a schedule (geometric waiting times of
+            // the per-step Bernoulli flips): the current barrier flips at its
+            // pending flip step; a barrier left keeps its pending flip in the
+            // cell table; one re-entered before that step has not flipped
+            // meanwhile (no draw); one whose flip came while it was away (or
+            // never visited: created at step 0) is caught up from that step
+            // with the two-state transition probability (S.h:2025-2068).
             const bool flip = (int64_t)s == nflip;
-            if (flip) t.state ^= 1;
-            const int st_flip = t.state;
-            if (dKey) {
-                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, (int64_t)s);
-                int ps;
-                int64_t stamp;
-                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &stamp);
-                const double lap = (double)((int64_t)s - stamp);
-                const double pl = k.c_lap[k.eq ? 0 : ps] * -expm1_f64(k.a_lap * lap);
-                const uint64_t Tl = prob_to_u64(pl);
-                const Words wc = philox_at(s, g, TAG_CATCHUP, k.key0, k.key1);
-                const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
-                t.state = (U < Tl) ? (ps ^ 1) : ps;
+            Words wf{};
+            bool have_wf = false;
+            if (flip) {
+                t.state ^= 1;
+                wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+                have_wf = true;
+                nflip = flip_schedule(s, wf.w0, wf.w1, k.ln1m[t.state]);
             }
-            // A pending waiting time stays valid across a barrier change
-            // whose flip probability is the same (memoryless).
-            if (flip || (dKey && k.ln1m[t.state] != k.ln1m[st_flip])) {
-                const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
-                const uint64_t wt = flip_wait(wf.w0, wf.w1, k.ln1m[t.state]);
-                nflip = (wt >= 0x7fffffffffffffffull - s) ? 0x7fffffffffffffffll : (int64_t)(s + wt);
+            if (dKey) {
+                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, nflip);
+                int ps;
+                int64_t nb;
+                bool found;
+                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &nb, &found);
+                if (found && nb > (int64_t)s) {
+                    t.state = ps;
+                    nflip = nb;
+                } else {
+                    const int64_t base = found ? nb : 0;
+                    const int sb = found ? (ps ^ 1) : ps;
+                    const double lap = (double)((int64_t)s - base);
+                    const double pl = k.c_lap[k.eq ? 0 : sb] * -expm1_f64(k.a_lap * lap);
+                    const uint64_t Tl = prob_to_u64(pl);
+                    const Words wc = philox_at(s, g, TAG_CATCHUP, k.key0, k.key1);
+                    const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
+                    t.state = (U < Tl) ? (sb ^ 1) : sb;
+                    if (!have_wf) wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+                    nflip = flip_schedule(s, wf.w2, wf.w3, k.ln1m[t.state]);
+                }
             }
         } else {
             // UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434.
             if (dKey) {
-                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, (int64_t)s);
+                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, nflip);
                 int ps;
-                int64_t stamp;
-                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &stamp);
+                int64_t nb;
+                bool found;
+                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &nb, &found);
                 t.state = ps;
             }
         }

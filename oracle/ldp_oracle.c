@@ -161,6 +161,12 @@ uint64_t ldpo_flip_wait(uint32_t hi, uint32_t lo, double ln1m) {
     return 1ull + (uint64_t)floor(q);
 }
 
+/* Step of the next flip drawn at step s: s + W, clamped to LDPO_NEVER. */
+int64_t ldpo_schedule(uint64_t s, uint32_t hi, uint32_t lo, double ln1m) {
+    const uint64_t wt = ldpo_flip_wait(hi, lo, ln1m);
+    return (wt >= (uint64_t)LDPO_NEVER - s) ? LDPO_NEVER : (int64_t)(s + wt);
+}
+
 uint64_t ldpo_prob_to_u64(double p) {
     if (!(p > 0.0)) return 0;
     if (p >= 1.0) return UINT64_MAX;
@@ -381,30 +387,36 @@ static int default_state(const ocst *k, const ldpo_cfg *c, const ldp_params *p, 
     return ((double)w[0] * 0x1p-32 < k->p_cell0) ? 0 : 1;   /* S.h:90-94 */
 }
 
+/* A cell-table entry: the barrier's state when it was left and its pending
+ * flip step (the first flip after it was left); *found = 0 for a cell never
+ * visited (state drawn as at creation, step 0: m_UserData.m_iStep stays 0,
+ * S.h:1375). */
 static void ring_load(const ocst *k, const ldpo_cfg *c, const ldp_params *p, const uint32_t key[2], uint32_t g,
-                      ring *r, int64_t ck, int *state, int64_t *stamp) {
+                      ring *r, int64_t ck, int *state, int64_t *nflip, int *found) {
     int slot = (int)(ck & (r->slots - 1));
     if (r->tag[slot] == ck) {
         *state = (int)(r->data[slot] & 1);
-        *stamp = r->data[slot] >> 1;
+        *nflip = r->data[slot] >> 1;
+        *found = 1;
     } else {
         *state = default_state(k, c, p, key, g, ck);
-        *stamp = 0;   /* m_UserData.m_iStep stays 0, S.h:1375 */
+        *nflip = 0;
+        *found = 0;
     }
 }
 
-static void ring_store(ring *r, int64_t ck, int state, int64_t stamp, int64_t *evict) {
+static void ring_store(ring *r, int64_t ck, int state, int64_t nflip, int64_t *evict) {
     int slot = (int)(ck & (r->slots - 1));
     if (r->tag[slot] != ck && r->tag[slot] != INT64_MIN) ++*evict;
     r->tag[slot] = ck;
-    r->data[slot] = (stamp << 1) | state;
+    r->data[slot] = (nflip << 1) | state;
 }
 
 static int table_state(const ocst *k, const ldpo_cfg *c, const ldp_params *p, const uint32_t key[2], uint32_t g,
                        ring *r, int64_t cell) {
-    int st;
-    int64_t stamp;
-    ring_load(k, c, p, key, g, r, cell_key(k, cell, 0), &st, &stamp);
+    int st, found;
+    int64_t nf;
+    ring_load(k, c, p, key, g, r, cell_key(k, cell, 0), &st, &nf, &found);
     return st;
 }
 
@@ -547,8 +559,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
         {
             uint32_t wf[4];
             philox_at(0, g, TAG_FLIP, key, wf);
-            const uint64_t wt = ldpo_flip_wait(wf[0], wf[1], k->ln1m[t.state]);
-            nflip = (wt == UINT64_MAX) ? INT64_MAX : (int64_t)wt;
+            nflip = ldpo_schedule(0, wf[0], wf[1], k->ln1m[t.state]);
         }
         energy_force(k, &t);
         /* InitializeStatistics, S.h:2166-2333 */
@@ -620,40 +631,52 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
             const int dKey = k->dbl ? (t.lb != lb_prev) : dCell;
 
             if (k->eta) {
-                /* UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736: the
-                 * current barrier flips at its scheduled step; a flip or a
-                 * barrier change schedules the next one (below). */
+                /* UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736, with
+                 * every barrier's flips on a schedule: the current barrier
+                 * flips at its pending flip step; a barrier left keeps its
+                 * pending flip in the cell table; one re-entered before that
+                 * step has not flipped meanwhile (no draw), one whose flip
+                 * came while it was away (or never visited: created at step
+                 * 0) is caught up from that step with the two-state
+                 * transition probability (S.h:2025-2068). */
                 const int flip = (int64_t)s == nflip;
-                if (flip) t.state ^= 1;
-                const int st_flip = t.state;
-                if (dKey) {
-                    ring_store(&r, cell_key(k, cell_prev, lb_prev), t.state, (int64_t)s, &evict);
-                    int ps;
-                    int64_t stamp;
-                    ring_load(k, c, p, key, g, &r, cell_key(k, t.cell, t.lb), &ps, &stamp);
-                    double lap = (double)((int64_t)s - stamp);
-                    double pl = k->c_lap[k->eq ? 0 : ps] * -ldpo_expm1(k->a_lap * lap);
-                    uint64_t Tl = ldpo_prob_to_u64(pl);
-                    uint32_t wc[4];
-                    philox_at(s, g, TAG_CATCHUP, key, wc);
-                    uint64_t U = ((uint64_t)wc[0] << 32) | wc[1];
-                    t.state = (U < Tl) ? (ps ^ 1) : ps;
-                }
-                /* A pending waiting time stays valid across a barrier change
-                 * whose flip probability is the same (memoryless). */
-                if (flip || (dKey && k->ln1m[t.state] != k->ln1m[st_flip])) {
-                    uint32_t wf[4];
+                uint32_t wf[4];
+                int have_wf = 0;
+                if (flip) {
+                    t.state ^= 1;
                     philox_at(s, g, TAG_FLIP, key, wf);
-                    const uint64_t wt = ldpo_flip_wait(wf[0], wf[1], k->ln1m[t.state]);
-                    nflip = (wt >= (uint64_t)INT64_MAX - s) ? INT64_MAX : (int64_t)(s + wt);
+                    have_wf = 1;
+                    nflip = ldpo_schedule(s, wf[0], wf[1], k->ln1m[t.state]);
+                }
+                if (dKey) {
+                    ring_store(&r, cell_key(k, cell_prev, lb_prev), t.state, nflip, &evict);
+                    int ps, found;
+                    int64_t nb;
+                    ring_load(k, c, p, key, g, &r, cell_key(k, t.cell, t.lb), &ps, &nb, &found);
+                    if (found && nb > (int64_t)s) {
+                        t.state = ps;
+                        nflip = nb;
+                    } else {
+                        const int64_t base = found ? nb : 0;
+                        const int sb = found ? (ps ^ 1) : ps;
+                        double lap = (double)((int64_t)s - base);
+                        double pl = k->c_lap[k->eq ? 0 : sb] * -ldpo_expm1(k->a_lap * lap);
+                        uint64_t Tl = ldpo_prob_to_u64(pl);
+                        uint32_t wc[4];
+                        philox_at(s, g, TAG_CATCHUP, key, wc);
+                        uint64_t U = ((uint64_t)wc[0] << 32) | wc[1];
+                        t.state = (U < Tl) ? (sb ^ 1) : sb;
+                        if (!have_wf) philox_at(s, g, TAG_FLIP, key, wf);
+                        nflip = ldpo_schedule(s, wf[2], wf[3], k->ln1m[t.state]);
+                    }
                 }
             } else {
                 /* UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434 */
                 if (dKey) {
-                    ring_store(&r, cell_key(k, cell_prev, lb_prev), t.state, (int64_t)s, &evict);
-                    int ps;
-                    int64_t stamp;
-                    ring_load(k, c, p, key, g, &r, cell_key(k, t.cell, t.lb), &ps, &stamp);
+                    ring_store(&r, cell_key(k, cell_prev, lb_prev), t.state, nflip, &evict);
+                    int ps, found;
+                    int64_t nb;
+                    ring_load(k, c, p, key, g, &r, cell_key(k, t.cell, t.lb), &ps, &nb, &found);
                     t.state = ps;
                 }
             }

@@ -35,6 +35,9 @@ void     ldpo_sincos2pi(double t, double *s, double *c);
 double   ldpo_expm1(double x);
 uint64_t ldpo_prob_to_u64(double p);
 uint64_t ldpo_flip_wait(uint32_t hi, uint32_t lo, double ln1m);
+/* "Never" for a flip step: fits the cell table's (step << 1 | state). */
+#define LDPO_NEVER ((int64_t)((1ull << 62) - 1))
+int64_t  ldpo_schedule(uint64_t s, uint32_t hi, uint32_t lo, double ln1m);
 
 /* Steps integrated per trajectory and frames recorded, as the reference's
  * Integrate loop does them (S.h:1403-1511). */

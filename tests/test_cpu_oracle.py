@@ -117,3 +117,55 @@ def test_every_sample_input_parses(name):
     p = ldp.params_from_inp(os.path.join(GOLDEN, "inp", name), model)
     assert p.number_of_steps > 0 and p.timestep > 0
     assert p.model == model
+
+
+def free_barrier_params(eq, K, tau, nsteps):
+    """Zero barrier heights (no force: the cells a trajectory visits do not
+    depend on the barrier states), every barrier in state 0 at step 0, fast
+    diffusion (a cell change every few hundred steps, revisits common)."""
+    p = quick_params()
+    bh = p.barrier_heights
+    for i in range(len(bh)):
+        for j in range(len(bh[i])):
+            bh[i][j] = 0.0
+    p.temperature = 400.0
+    p.tau, p.eq, p.eq_constant = tau, int(eq), K
+    p.initial_state, p.randomize_states, p.uniform_initial_states = 0, 0, 1
+    p.number_of_steps, p.freq_save = nsteps, nsteps // 10
+    p.write_x = p.waiting_time = p.tpt = 0
+    p.fptcg = p.n_cg = 0
+    return p
+
+
+def expected_state1_steps(eq, K, tau, dt, n):
+    """Mean steps in state 1 over steps 0..n of a two-state chain started in
+    state 0, flip probabilities a (0->1) and b (1->0) per step: the state at
+    step k is 1 with probability pi1 (1 - lam^k), lam = 1 - a - b."""
+    if eq:
+        lam, pi1 = np.exp(-2.0 * dt / tau), 0.5
+    else:
+        lam, pi1 = np.exp(-(K + 1.0) * dt / tau), K / (1.0 + K)
+    return pi1 * ((n + 1) - (1.0 - lam ** (n + 1)) / (1.0 - lam))
+
+
+@pytest.mark.parametrize("eq,K,tau", [(True, 1.0, 1.0), (False, 3.0, 2.0)])
+def test_unobserved_barriers_follow_the_two_state_chain(eq, K, tau):
+    # Each barrier flips as an independent two-state chain whether or not the
+    # trajectory is in its cell: the current barrier on its pending flip
+    # steps, a barrier left and re-entered by its kept pending flip or the
+    # closed-form catch-up.  With no force the observed barrier's state at
+    # step k is 1 with probability pi1 (1 - lam^k) whatever cells were
+    # visited, so the mean time in state 1 has a closed form.
+    n = 10_000
+    p = free_barrier_params(eq, K, tau, n)
+    r = O.run(p, 4321, lanes=8192, frames=False)
+    c = r["counts"]
+    assert np.all(r["state0"] == 0)
+    assert np.all(c[L.C_EVICT] == 0)
+    assert c[L.C_FPT2].mean() > 15          # many well-to-well passages each
+    s1 = c[L.C_STATE1].astype(np.float64)
+    want = expected_state1_steps(eq, K, tau, p.timestep, n)
+    se = s1.std() / np.sqrt(len(s1))
+    print(f"state-1 steps: {s1.mean():.1f} +- {se:.1f}, chain {want:.1f}")
+    assert abs(s1.mean() - want) < 4 * se
+    assert se < 0.006 * want

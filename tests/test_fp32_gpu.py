@@ -177,3 +177,37 @@ def test_fp32_first_passage_distribution_matches_fp64(ctx):
     assert ks.pvalue > 0.01
     se = np.sqrt(ta.var() / len(ta) + tb.var() / len(tb))
     assert abs(ta.mean() - tb.mean()) < 3 * se
+
+
+@pytest.mark.parametrize("dbl", [False, True])
+@pytest.mark.parametrize("eq,K,tau", [(True, 1.0, 1.0), (False, 3.0, 2.0)])
+@pytest.mark.parametrize("precision", [ldp.PREC_FP64_PLAIN, ldp.PREC_FP32_BATCHED])
+def test_unobserved_barriers_follow_the_two_state_chain(ctx, precision, eq, K, tau, dbl):
+    # Zero barrier heights (the cells visited do not depend on the barrier
+    # states), every barrier in state 0 at step 0, a cell change every few
+    # hundred steps.  Each barrier flips as an independent two-state chain
+    # whether observed or not, so the observed barrier is in state 1 at step
+    # k with probability pi1 (1 - lam^k), lam = 1 - a - b for flip
+    # probabilities a (0->1) and b (1->0): the mean time in state 1 over
+    # 65536 trajectories is within 4 standard errors of the closed form.
+    n = 10_000
+    p = (double if dbl else quick)(steps=n, freq=5)     # 2001 frames, 89 MSD lags
+    bh = p.barrier_heights
+    for i in range(len(bh)):
+        for j in range(len(bh[i])):
+            bh[i][j] = 0.0
+    p.temperature, p.tau, p.eq, p.eq_constant = 400.0, tau, int(eq), K
+    p.initial_state, p.randomize_states, p.uniform_initial_states = 0, 0, 1
+    p.write_x = p.waiting_time = p.tpt = 0
+    p.fptcg = p.n_cg = 0
+    r = run(ctx, p, precision, lanes=65536)
+    c = r["counts"]
+    assert np.all(r["state0"] == 0)
+    assert np.all(c[L.C_EVICT] == 0)
+    assert c[L.C_FPT2].mean() > 15
+    lam, pi1 = (np.exp(-2.0 * p.timestep / tau), 0.5) if eq else (np.exp(-(K + 1.0) * p.timestep / tau), K / (1 + K))
+    want = pi1 * ((n + 1) - (1.0 - lam ** (n + 1)) / (1.0 - lam))
+    s1 = c[L.C_STATE1].astype(np.float64)
+    se = s1.std() / np.sqrt(len(s1))
+    print(f"state-1 steps: {s1.mean():.2f} +- {se:.2f}, chain {want:.2f}")
+    assert abs(s1.mean() - want) < 4 * se
