@@ -128,6 +128,12 @@ typedef struct ldp_job_opts {
     int32_t keep_frames;      /* keep x frames on the device after the MSD
                                  (needed for ldp_job_traj_results frames);
                                  default 1                                   */
+    int32_t pad;
+    int64_t event_cap;        /* per-event lists kept per trajectory and list
+                                 (ldp_event_list; FP64 plain, fixed steps):
+                                 the reference's per-lane event vectors that
+                                 its .restart files hold.  0 = none (default);
+                                 -1 = automatic when WRITERESTART is set     */
 } ldp_job_opts;
 
 /* Per-trajectory counters, laid out [field][ntraj]. */
@@ -164,6 +170,16 @@ enum ldp_sum_field {
 #define LDP_FLAG_NONFINITE 1u   /* x became NaN/inf; trajectory frozen        */
 #define LDP_FLAG_TICK_OVERFLOW 2u /* more waiting ticks than tick_cap          */
 #define LDP_FLAG_CENSORED 4u    /* FIRST_PASSAGE: step_cap reached, no event  */
+#define LDP_FLAG_EVENT_OVERFLOW 8u /* more events in a list than event_cap   */
+
+/* Per-event lists (event durations in time units, event order), laid out
+ * [list][ntraj][event_cap]: m_FirstPassageTime{,2}, m_TransitionPathTime{,2}
+ * and m_FirstPassageTimeCG2 of each FPTCG entry
+ * (src/langevinDynamicsSingleBarrier.h:2352-2590). */
+enum ldp_event_list {
+    LDP_E_FPT = 0, LDP_E_FPT2, LDP_E_TPT, LDP_E_TPT2,
+    LDP_E_CG0          /* LDP_E_CG0 + j for FPTCG entry j; LDP_E_CG0 + n_cg lists */
+};
 
 typedef struct ldp_job_info {
     int64_t ntraj;        /* trajectories                                   */
@@ -176,6 +192,8 @@ typedef struct ldp_job_info {
     int32_t mode;
     int32_t done;
     int64_t device_bytes; /* device memory the job holds while it runs      */
+    int64_t event_cap;    /* events kept per trajectory and list            */
+    int64_t steps_before; /* steps restored from a restart (0: fresh start) */
 } ldp_job_info;
 
 /*
@@ -194,6 +212,11 @@ typedef struct ldp_traj_results {
     double  *frames_x;      /* [nframe][ntraj]                              */
     double  *frames_v, *frames_f, *frames_barrier, *frames_pe, *frames_ke,
             *frames_state;  /* WRITEX series, [nframe][ntraj]               */
+    double  *events;        /* [LDP_E_CG0 + n_cg][ntraj][event_cap]         */
+    uint8_t *event_states;  /* [ntraj][event_cap]: per FPT event, bit 0 the
+                               instantaneous and bit 1 the initial barrier
+                               state (m_InstantBarrierList,
+                               m_InitialBarrierList, S.h:2396-2404)         */
 } ldp_traj_results;
 
 typedef struct ldp_timing {
@@ -354,6 +377,44 @@ ldp_status  ldp_job_write_outputs(ldp_job *job, const char *dir);
 ldp_status  ldp_integrate_fp64_noalloc(const ldp_params *p, const ldp_job_opts *o, int64_t *d_counts,
                                        double *d_sums, double *d_x_final, double *d_frames_x,
                                        void *stream, char *err, size_t errlen);
+
+/*
+ * Restart files (READRESTART / WRITERESTART / INPUTRESTART / OUTPUTRESTART):
+ * one file per virtual rank and trial, <base>_%05d_%05d.restart, in the
+ * layout of LangevinEquationSIMDMultiple::Write/ReadRestartFile
+ * (src/langevinDynamicsSingleBarrier.h:385-820, 1048-1275;
+ * src/langevinDynamicsDoubleBarrier.h:414-932, 1202-1447), FP64 plain jobs
+ * in fixed-step mode.  ldp_job_restore loads the files into a created job
+ * before ldp_submit (the job's NUMBEROFPREVIOUSSTEPS must equal the steps
+ * the files hold; NUMBEROFSTEPS more steps follow, frames and statistics
+ * continue the file's); ldp_job_save_restart writes them after the run
+ * (the job needs event_cap > 0: the files hold every event).  Files written
+ * here carry, after the reference's trailer, a block that makes a resumed
+ * run equal the uninterrupted one bit for bit; files the reference wrote
+ * resume with the same statistics (the barrier flips' pending steps are
+ * drawn from the job's streams).
+ */
+typedef struct ldp_restart_summary {
+    int32_t lanes;            /* SIMDWIDTH of the writer (lanes per file)    */
+    int32_t rank;             /* the writer's rank                           */
+    uint64_t steps;           /* steps done                                  */
+    int64_t frames;           /* frames of the x series                      */
+    int32_t has_exact_resume; /* written by this library                     */
+    int32_t pad;
+    int64_t ncell[2];         /* barrier-table cells (double model: two)     */
+    int32_t min_id[2];        /* first cell index of each table              */
+} ldp_restart_summary;
+ldp_status  ldp_job_restore(ldp_job *job, const char *input_base);
+ldp_status  ldp_job_save_restart(ldp_job *job, const char *output_base);
+/* One file: its summary and, optionally, the per-lane counts and sums a
+ * job restored from it starts with ([LDP_NCOUNT][lanes], [LDP_NSUM][lanes]).
+ * p selects the layout (model, OVERDAMPED, TPT, FPTCG). */
+ldp_status  ldp_restart_inspect(const ldp_params *p, const char *path, ldp_restart_summary *s,
+                                int64_t *counts, double *sums, char *err, size_t errlen);
+/* Reads a file and writes it again (a byte-identical copy for a file of
+ * the same layout): validates a file against the layout. */
+ldp_status  ldp_restart_rewrite(const ldp_params *p, const char *in, const char *out, char *err,
+                                size_t errlen);
 
 /* One-shot drop-in for `mpirun -n ranks ./exe -i path`. */
 ldp_status  ldp_run_inp(ldp_ctx *ctx, const char *path, int model,

@@ -18,7 +18,7 @@ from ._lib import (MODEL_SINGLE, MODEL_DOUBLE, PREC_FP64_PLAIN, PREC_FP32_BATCHE
                    MODE_FIXED_STEPS, MODE_FIRST_PASSAGE, LdpError, Params, JobOpts)
 
 __all__ = ["Context", "Job", "default_params", "params_from_inp", "params_from_inp_text",
-           "MODEL_SINGLE", "MODEL_DOUBLE", "LdpError"]
+           "restart_inspect", "restart_rewrite", "MODEL_SINGLE", "MODEL_DOUBLE", "LdpError"]
 
 
 def _check(st: int, ctx=None):
@@ -88,13 +88,13 @@ class Job:
     def __init__(self, ctx: Context, params: Params, lanes: int = 8, ranks: int = 1,
                  precision: int = PREC_FP64_PLAIN, mode: int = MODE_FIXED_STEPS,
                  step_cap: int = 100_000_000, table_slots: int = 256, tick_cap: int = -1,
-                 job_id: int = 0, steps_per_launch: int = 0, block_size: int = 0):
+                 job_id: int = 0, steps_per_launch: int = 0, block_size: int = 0, event_cap: int = 0):
         self.ctx = ctx
         o = JobOpts()
         L.lib().ldp_job_opts_default(C.byref(o))
         o.lanes, o.ranks, o.precision, o.mode = lanes, ranks, precision, mode
         o.step_cap, o.table_slots, o.tick_cap, o.job_id = step_cap, table_slots, tick_cap, job_id
-        o.steps_per_launch, o.block_size = steps_per_launch, block_size
+        o.steps_per_launch, o.block_size, o.event_cap = steps_per_launch, block_size, event_cap
         self.opts = o
         self.params = params
         h = C.c_void_p()
@@ -127,6 +127,19 @@ class Job:
 
     def run(self) -> "Job":
         return self.submit().wait()
+
+    # -- restart files (ReadRestartFile / WriteRestartFile) -----------------
+    def restore(self, input_base: str) -> "Job":
+        """Loads <input_base>_<rank>_<trial>.restart before submission; the
+        params' NUMBEROFPREVIOUSSTEPS must equal the files' step count."""
+        _check(L.lib().ldp_job_restore(self.handle, input_base.encode()), self.ctx)
+        return self
+
+    def save_restart(self, output_base: str) -> "Job":
+        """Writes <output_base>_<rank>_<trial>.restart after the run (needs
+        event_cap > 0, or -1 with WRITERESTART true)."""
+        _check(L.lib().ldp_job_save_restart(self.handle, output_base.encode()), self.ctx)
+        return self
 
     # -- introspection -----------------------------------------------------
     @property
@@ -164,6 +177,11 @@ class Job:
         if ticks and tc > 0:
             out["ticks"] = np.zeros((n, tc), np.int64)
             r.ticks = _ptr(out["ticks"], C.c_int64)
+        if i.event_cap > 0:
+            out["events"] = np.zeros((L.E_CG0 + i.n_cg, n, i.event_cap), np.float64)
+            out["event_states"] = np.zeros((n, i.event_cap), np.uint8)
+            r.events = _ptr(out["events"], C.c_double)
+            r.event_states = _ptr(out["event_states"], C.c_uint8)
         if frames and nf > 0:
             out["frames_x"] = np.zeros((nf, n), np.float64)
             r.frames_x = _ptr(out["frames_x"], C.c_double)
@@ -200,6 +218,33 @@ class Job:
 
     def __exit__(self, *a):
         self.close()
+
+
+def restart_inspect(params: Params, path: str) -> dict:
+    """Summary of one .restart file and the per-lane counts and sums a job
+    restored from it starts with (ldp_restart_inspect)."""
+    s = L.RestartSummary()
+    err = C.create_string_buffer(1024)
+    st = L.lib().ldp_restart_inspect(C.byref(params), path.encode(), C.byref(s), None, None, err, 1024)
+    if st != 0:
+        raise LdpError(st, err.value.decode())
+    counts = np.zeros((L.NCOUNT, s.lanes), np.int64)
+    sums = np.zeros((L.NSUM, s.lanes), np.float64)
+    st = L.lib().ldp_restart_inspect(C.byref(params), path.encode(), C.byref(s), _ptr(counts, C.c_int64),
+                                     _ptr(sums, C.c_double), err, 1024)
+    if st != 0:
+        raise LdpError(st, err.value.decode())
+    return {"lanes": s.lanes, "rank": s.rank, "steps": s.steps, "frames": s.frames,
+            "has_exact_resume": bool(s.has_exact_resume), "ncell": list(s.ncell), "min_id": list(s.min_id),
+            "counts": counts, "sums": sums}
+
+
+def restart_rewrite(params: Params, src: str, dst: str) -> None:
+    """Reads a .restart file and writes it again (ldp_restart_rewrite)."""
+    err = C.create_string_buffer(1024)
+    st = L.lib().ldp_restart_rewrite(C.byref(params), src.encode(), dst.encode(), err, 1024)
+    if st != 0:
+        raise LdpError(st, err.value.decode())
 
 
 def submit_batch(ctx: Context, jobs, graph: bool = False) -> None:

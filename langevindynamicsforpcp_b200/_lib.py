@@ -26,7 +26,9 @@ NCOUNT = C_CG0 + LDP_MAX_CG
 S_FPT, S_FPT2, S_TPT, S_TPT2, S_FIRST_FPT, S_FIRST_FPT2, S_FIRST_TPT, S_FIRST_TPT2, S_CG0 = range(9)
 NSUM = S_CG0 + LDP_MAX_CG
 
-FLAG_NONFINITE, FLAG_TICK_OVERFLOW, FLAG_CENSORED = 1, 2, 4
+FLAG_NONFINITE, FLAG_TICK_OVERFLOW, FLAG_CENSORED, FLAG_EVENT_OVERFLOW = 1, 2, 4, 8
+# enum ldp_event_list
+E_FPT, E_FPT2, E_TPT, E_TPT2, E_CG0 = range(5)
 NOALLOC_MAX_TRAJ = 4096
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "device error", 4: "timeout",
@@ -68,14 +70,15 @@ class JobOpts(C.Structure):
         ("lanes", C.c_int32), ("ranks", C.c_int32), ("precision", C.c_int32), ("mode", C.c_int32),
         ("step_cap", C.c_uint64), ("table_slots", C.c_int32), ("tick_cap", C.c_int64),
         ("job_id", C.c_uint32), ("steps_per_launch", C.c_uint64), ("block_size", C.c_int32),
-        ("keep_frames", C.c_int32),
+        ("keep_frames", C.c_int32), ("pad", C.c_int32), ("event_cap", C.c_int64),
     ]
 
 
 class JobInfo(C.Structure):
     _fields_ = [("ntraj", C.c_int64), ("nframe", C.c_int64), ("nlag", C.c_int64), ("steps", C.c_int64),
                 ("tick_cap", C.c_int64), ("n_cg", C.c_int32), ("precision", C.c_int32), ("mode", C.c_int32),
-                ("done", C.c_int32), ("device_bytes", C.c_int64)]
+                ("done", C.c_int32), ("device_bytes", C.c_int64), ("event_cap", C.c_int64),
+                ("steps_before", C.c_int64)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -87,7 +90,14 @@ class TrajResults(C.Structure):
     _fields_ = [("counts", _I64P), ("sums", _DP), ("state0", _I32P), ("v0", _DP), ("x_final", _DP),
                 ("v_final", _DP), ("state_final", _I32P), ("ticks", _I64P), ("frames_x", _DP),
                 ("frames_v", _DP), ("frames_f", _DP), ("frames_barrier", _DP), ("frames_pe", _DP),
-                ("frames_ke", _DP), ("frames_state", _DP)]
+                ("frames_ke", _DP), ("frames_state", _DP), ("events", _DP),
+                ("event_states", C.POINTER(C.c_uint8))]
+
+
+class RestartSummary(C.Structure):
+    _fields_ = [("lanes", C.c_int32), ("rank", C.c_int32), ("steps", C.c_uint64), ("frames", C.c_int64),
+                ("has_exact_resume", C.c_int32), ("pad", C.c_int32), ("ncell", C.c_int64 * 2),
+                ("min_id", C.c_int32 * 2)]
 
 
 class ServerOpts(C.Structure):
@@ -154,6 +164,11 @@ SIGNATURES = {
     "ldp_server_destroy": (None, [C.c_void_p]),
     "ldp_integrate_fp64_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(JobOpts), C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),
+    "ldp_job_restore": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ldp_job_save_restart": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ldp_restart_inspect": (C.c_int, [C.POINTER(Params), C.c_char_p, C.POINTER(RestartSummary), _I64P, _DP,
+                                      C.c_char_p, C.c_size_t]),
+    "ldp_restart_rewrite": (C.c_int, [C.POINTER(Params), C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None

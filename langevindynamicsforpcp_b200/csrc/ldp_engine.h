@@ -38,7 +38,7 @@ struct KConst {
     double ln1m[2];          // log(1 - per-step flip probability) by state; 0: never flips
     double a_lap, c_lap[2], p_first, p_cell0;
     uint64_t nsteps, freq_save, step_cap;
-    int64_t nframe, tick_cap;
+    int64_t nframe, tick_cap, ev_cap;
     // FP32 cell-local copies (FP32 batched path)
     float fL, fhalfL, fw, fslope[2], fxb[2], flo0, fhi1, fxc;
     float fsN[2][2], fsP[2][2];
@@ -61,6 +61,8 @@ struct TrajState {
     double *v0;
     int64_t *ring_tag, *ring_data;  // [slots][n]
     int64_t *ticks;     // [n][tick_cap]
+    double *ev;         // per-event lists [LDP_E_CG0 + n_cg][n][ev_cap]
+    uint8_t *ev_st;     // FPT event barrier states [n][ev_cap]
     double *fx, *fv, *ff, *fb, *fpe, *fke, *fst;  // frames [nframe][n]
 };
 

@@ -215,6 +215,7 @@ __device__ __noinline__ void f_record_extra(const JobF* Jp, int64_t o, float xp,
 template <bool DBL>
 __device__ __forceinline__ void f_record(const JobF& J, uint32_t traj, int64_t frame, int cell, float xp, float v,
                                          float F, int state) {
+    if (frame >= J.nframe) return;   // the frame arrays hold nframe rows
     const int64_t o = frame * J.ntraj + traj;
     if (J.fx) J.fx[o] = (double)cell * J.Ld + (double)xp;
     if (J.write_x) f_record_extra<DBL>(&J, o, xp, v, F, state);

@@ -163,8 +163,18 @@ __device__ __forceinline__ void fpt2_set_idx(T64& t) {
 
 __device__ __forceinline__ bool cg_hit(int64_t well, int size) { return ((int)well % size) == 0; }
 
+// Appends an event duration to list `list` of trajectory i (the reference's
+// push_back on its per-lane vectors, S.h:2391, 2447, 2504, 2524, 2580); c is
+// the list's count before the event.  A full list flags the trajectory.
+__device__ __noinline__ void ev_push(const KConst& k, const TrajState& st, int list, int64_t i, int64_t c, double d,
+                                     uint32_t* flags) {
+    if (c < k.ev_cap) st.ev[((int64_t)list * st.n + i) * k.ev_cap + c] = d;
+    else *flags |= LDP_FLAG_EVENT_OVERFLOW;
+}
+
 __device__ __forceinline__ void record(const KConst& k, const TrajState& st, const T64& t, int64_t i,
                                        int64_t frame) {
+    if (frame >= k.nframe) return;   // the frame arrays hold nframe rows
     const int64_t o = frame * st.n + i;
     if (st.fx) st.fx[o] = t.x;
     if (k.write_x) {
@@ -390,11 +400,16 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
                     }
                     if (!(t.bits & B_FPT_UP) && dWell) {
                         t.bits |= B_FPT_UP;
-                        if (st.counts[(int64_t)LDP_C_FPT * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_FPT * n + i] = now - t.fpt_last;
+                        const int64_t c = st.counts[(int64_t)LDP_C_FPT * n + i];
+                        if (c == 0) st.sums[(int64_t)LDP_S_FIRST_FPT * n + i] = now - t.fpt_last;
                         st.sums[(int64_t)LDP_S_FPT * n + i] += now - t.fpt_last;
-                        st.counts[(int64_t)LDP_C_FPT * n + i] += 1;
+                        st.counts[(int64_t)LDP_C_FPT * n + i] = c + 1;
                         const bool ib = ((double)t.cell == (double)t.init_idx0) ? ((t.bits & B_INIT0) != 0)
                                                                                 : ((t.bits & B_INIT1) != 0);
+                        if (k.ev_cap) {
+                            ev_push(k, st, LDP_E_FPT, i, c, now - t.fpt_last, &flags);
+                            if (c < k.ev_cap) st.ev_st[i * k.ev_cap + c] = (uint8_t)((t.state ? 1 : 0) | (ib ? 2 : 0));
+                        }
                         st.counts[(int64_t)(ib ? LDP_C_INIT1 : LDP_C_INIT0) * n + i] += 1;
                         st.counts[(int64_t)(t.state ? LDP_C_INST1 : LDP_C_INST0) * n + i] += 1;
                     }
@@ -405,9 +420,11 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
                     fpt2_set_idx(t);
                 }
                 if (dCell && !(t.bits & B_FPT2_UP) && t.idx2_0 != t.cell && t.idx2_1 != t.cell) {
-                    if (st.counts[(int64_t)LDP_C_FPT2 * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_FPT2 * n + i] = now - t.fpt2_last;
+                    const int64_t c = st.counts[(int64_t)LDP_C_FPT2 * n + i];
+                    if (c == 0) st.sums[(int64_t)LDP_S_FIRST_FPT2 * n + i] = now - t.fpt2_last;
                     st.sums[(int64_t)LDP_S_FPT2 * n + i] += now - t.fpt2_last;
-                    st.counts[(int64_t)LDP_C_FPT2 * n + i] += 1;
+                    st.counts[(int64_t)LDP_C_FPT2 * n + i] = c + 1;
+                    if (k.ev_cap) ev_push(k, st, LDP_E_FPT2, i, c, now - t.fpt2_last, &flags);
                     t.fpt2_last = now;
                     fpt2_set_idx(t);
                     if (k.fp_mode) t.bits |= B_DONE;   // first passage reached
@@ -417,16 +434,20 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
                 if (dCell) { t.bits &= ~B_TPT_UP; t.tpt_last = now; }
                 if (!(t.bits & B_TPT_UP) && dWell) {
                     t.bits |= B_TPT_UP;
-                    if (st.counts[(int64_t)LDP_C_TPT * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_TPT * n + i] = now - t.tpt_last;
+                    const int64_t c = st.counts[(int64_t)LDP_C_TPT * n + i];
+                    if (c == 0) st.sums[(int64_t)LDP_S_FIRST_TPT * n + i] = now - t.tpt_last;
                     st.sums[(int64_t)LDP_S_TPT * n + i] += now - t.tpt_last;
-                    st.counts[(int64_t)LDP_C_TPT * n + i] += 1;
+                    st.counts[(int64_t)LDP_C_TPT * n + i] = c + 1;
+                    if (k.ev_cap) ev_push(k, st, LDP_E_TPT, i, c, now - t.tpt_last, &flags);
                 }
                 if (dCell) {
                     if (t.bits & B_TPT2_UP) t.bits &= ~B_TPT2_UP;
                     else if (t.well != t.tpt2_well) {
-                        if (st.counts[(int64_t)LDP_C_TPT2 * n + i] == 0) st.sums[(int64_t)LDP_S_FIRST_TPT2 * n + i] = now - t.tpt2_last;
+                        const int64_t c = st.counts[(int64_t)LDP_C_TPT2 * n + i];
+                        if (c == 0) st.sums[(int64_t)LDP_S_FIRST_TPT2 * n + i] = now - t.tpt2_last;
                         st.sums[(int64_t)LDP_S_TPT2 * n + i] += now - t.tpt2_last;
-                        st.counts[(int64_t)LDP_C_TPT2 * n + i] += 1;
+                        st.counts[(int64_t)LDP_C_TPT2 * n + i] = c + 1;
+                        if (k.ev_cap) ev_push(k, st, LDP_E_TPT2, i, c, now - t.tpt2_last, &flags);
                     }
                     t.tpt2_last = now;
                     t.tpt2_well = t.well;
@@ -442,7 +463,9 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
                             st.cg_well[o] = t.well;
                         } else if (t.well != st.cg_well[o]) {
                             st.sums[(int64_t)(LDP_S_CG0 + jj) * n + i] += now - st.cg_last[o];
-                            st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i] += 1;
+                            const int64_t c = st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i];
+                            st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i] = c + 1;
+                            if (k.ev_cap) ev_push(k, st, LDP_E_CG0 + jj, i, c, now - st.cg_last[o], &flags);
                             st.cg_last[o] = now;
                             st.cg_well[o] = t.well;
                         }

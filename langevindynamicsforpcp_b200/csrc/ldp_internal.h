@@ -61,6 +61,10 @@ struct ldp_job {
     int64_t launches = 0;
     int64_t steps_total = 0;
     double wall_start = 0.0;
+    bool restored = false;       // state loaded by ldp_job_restore
+    uint64_t steps_before = 0;   // steps the restart files held
+    bool ev_auto = false;        // event_cap / tick_cap chosen by the library
+    bool tick_auto = false;
     int64_t particle_steps_done() const;
 };
 

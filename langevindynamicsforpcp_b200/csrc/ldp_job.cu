@@ -183,6 +183,7 @@ extern "C" void ldp_job_opts_default(ldp_job_opts* o) {
     o->steps_per_launch = 0;
     o->block_size = 0;
     o->keep_frames = 1;
+    o->event_cap = -1;
 }
 
 // ---------------------------------------------------------------------------
@@ -249,6 +250,15 @@ static ldp_status validate(ldp_ctx* ctx, const ldp_params& p, const ldp_job_opts
         ldp_set_error(ctx, "BARRIERHALFWIDTH must be positive");
         return LDP_ERR_INVALID;
     }
+    const bool plain = o.precision == LDP_PREC_FP64_PLAIN;
+    if (p.number_of_previous_steps && !(plain && fixed)) {
+        ldp_set_error(ctx, "NUMBEROFPREVIOUSSTEPS (a restart) needs the FP64 plain path in fixed-step mode");
+        return LDP_ERR_UNSUPPORTED;
+    }
+    if (o.event_cap > 0 && !(plain && fixed)) {
+        ldp_set_error(ctx, "per-event lists (event_cap) need the FP64 plain path in fixed-step mode");
+        return LDP_ERR_UNSUPPORTED;
+    }
     if (fixed) {
         const uint64_t nf = (p.number_of_steps + p.number_of_previous_steps) / p.freq_save + 1;
         if (nf < 1000) {
@@ -288,6 +298,9 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     const size_t o_sum = take(sizeof(double) * LDP_NSUM * n);
     const size_t o_ring = take(f32 ? 0 : sizeof(int64_t) * 2 * (size_t)job->o.table_slots * n);
     const size_t o_tick = take(sizeof(int64_t) * (size_t)std::max<int64_t>(job->o.tick_cap, 1) * n);
+    const size_t ev_elems = (size_t)std::max<int64_t>(job->o.event_cap, 0) * n;
+    const size_t o_ev = take(sizeof(double) * (LDP_E_CG0 + p->n_cg) * ev_elems);
+    const size_t o_evst = take(ev_elems);
     const size_t o_fr = take(sizeof(double) * (size_t)std::max<int64_t>(job->nframe, 1) * n * std::max(nser, 1));
     const size_t o_msd0 = take(sizeof(double) * (size_t)std::max<int64_t>(nlag, 1) * n);
     const size_t o_msd = take(sizeof(double) * (size_t)std::max<int64_t>(nlag, 1));
@@ -324,6 +337,8 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     S.ring_tag = f32 ? nullptr : (int64_t*)(a + o_ring);
     S.ring_data = f32 ? nullptr : S.ring_tag + (size_t)job->o.table_slots * n;
     S.ticks = (int64_t*)(a + o_tick);
+    S.ev = ev_elems ? (double*)(a + o_ev) : nullptr;
+    S.ev_st = ev_elems ? (uint8_t*)(a + o_evst) : nullptr;
     double* fr = (double*)(a + o_fr);
     const size_t fstride = (size_t)std::max<int64_t>(job->nframe, 1) * n;
     S.fx = fixed ? fr : nullptr;
@@ -388,6 +403,8 @@ static ldp_status job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_op
         }
     }
     int64_t n = job->ntraj;
+    job->ev_auto = job->o.event_cap < 0;
+    job->tick_auto = job->o.tick_cap < 0;
     const bool wt = p->waiting_time && p->model == LDP_MODEL_SINGLE && fixed;
     if (!wt) job->o.tick_cap = 0;
     else if (job->o.tick_cap < 0) {
@@ -395,8 +412,17 @@ static ldp_status job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_op
         int64_t b = std::max<int64_t>(64, ((int64_t)1 << 27) / n);
         job->o.tick_cap = std::min(a, b);
     }
+    if (job->o.event_cap < 0) {
+        // Enough for about one event per 10^4 steps (the quick_test model
+        // records one FPT event per ~4*10^5 steps), within 2^28 list entries.
+        const int64_t lists = LDP_E_CG0 + p->n_cg;
+        const int64_t a = std::max<int64_t>(64, (int64_t)(job->nsteps / 10000));
+        const int64_t b = std::max<int64_t>(64, ((int64_t)1 << 28) / (n * lists));
+        job->o.event_cap = (p->write_restart && fixed && opts.precision == LDP_PREC_FP64_PLAIN) ? std::min(a, b) : 0;
+    }
     prepare_kconst(job->p, job->o, job->seed, &job->k);
     job->k.tick_cap = job->o.tick_cap;
+    job->k.ev_cap = job->o.event_cap;
 
     const size_t need = job_arena(job, false);
     cudaSetDevice(ctx->device);
@@ -415,7 +441,11 @@ static ldp_status job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_op
 extern "C" ldp_status ldp_job_set_precision(ldp_job* job, int precision) {
     if (!job) return LDP_ERR_INVALID;
     if (precision != LDP_PREC_FP64_PLAIN && precision != LDP_PREC_FP32_BATCHED) return LDP_ERR_INVALID;
-    if (job->submitted) return LDP_ERR_INVALID;
+    if (job->submitted || job->arena) return LDP_ERR_INVALID;
+    if (precision == LDP_PREC_FP32_BATCHED && (job->o.event_cap > 0 || job->p.number_of_previous_steps)) {
+        ldp_set_error(job->ctx, "per-event lists and restarts need the FP64 plain path");
+        return LDP_ERR_UNSUPPORTED;
+    }
     job->o.precision = precision;
     return LDP_OK;
 }
@@ -443,6 +473,10 @@ extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
         ldp_set_error(ctx, "cudaMalloc of %zu bytes failed", job_arena(job, false));
         return LDP_ERR_NOMEM;
     }
+    if (job->p.number_of_previous_steps && !job->restored) {
+        ldp_set_error(ctx, "NUMBEROFPREVIOUSSTEPS > 0 continues a restart: call ldp_job_restore first");
+        return LDP_ERR_INVALID;
+    }
     job->submitted = true;
     job->launches = 0;
     if (job->o.precision == LDP_PREC_FP32_BATCHED) {
@@ -459,15 +493,21 @@ extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
         return LDP_OK;
     } else {
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[0], s));
-        int e = launch_fp64_init(job->k, job->st, 0, job->o.block_size, s);
-        if (e) {
-            ldp_set_error(ctx, "init launch failed: %s", cudaGetErrorString((cudaError_t)e));
-            return LDP_ERR_DEVICE;
+        int e = 0;
+        if (!job->restored) {
+            e = launch_fp64_init(job->k, job->st, 0, job->o.block_size, s);
+            if (e) {
+                ldp_set_error(ctx, "init launch failed: %s", cudaGetErrorString((cudaError_t)e));
+                return LDP_ERR_DEVICE;
+            }
+            ++job->launches;
         }
-        ++job->launches;
+        // Steps continue the restart's numbering (S.h:1420: iStep =
+        // m_NumberOfStepDonePreviously + ...): the streams are keyed by it.
         const uint64_t spl = auto_steps_per_launch(job);
-        for (uint64_t s0 = 1; s0 <= job->nsteps; s0 += spl) {
-            const uint64_t s1 = std::min<uint64_t>(s0 + spl, job->nsteps + 1);
+        const uint64_t first = job->steps_before + 1, last = job->steps_before + job->nsteps;
+        for (uint64_t s0 = first; s0 <= last; s0 += spl) {
+            const uint64_t s1 = std::min<uint64_t>(s0 + spl, last + 1);
             e = launch_fp64_steps(job->k, job->st, 0, s0, s1, job->o.block_size, s);
             if (e) {
                 ldp_set_error(ctx, "step launch failed: %s", cudaGetErrorString((cudaError_t)e));
@@ -576,6 +616,8 @@ extern "C" ldp_status ldp_job_info_get(const ldp_job* job, ldp_job_info* info) {
     info->mode = job->o.mode;
     info->done = job->done ? 1 : 0;
     info->device_bytes = (int64_t)job_arena(const_cast<ldp_job*>(job), false);
+    info->event_cap = job->o.event_cap;
+    info->steps_before = (int64_t)job->steps_before;
     return LDP_OK;
 }
 
@@ -641,6 +683,10 @@ extern "C" ldp_status ldp_job_traj_results(ldp_job* job, ldp_traj_results* r) {
     CP(r->v_final, S.v, sizeof(double) * n);
     CP(r->state_final, S.state, sizeof(int32_t) * n);
     if (job->o.tick_cap > 0) CP(r->ticks, S.ticks, sizeof(int64_t) * job->o.tick_cap * n);
+    if (job->o.event_cap > 0) {
+        CP(r->events, S.ev, sizeof(double) * (LDP_E_CG0 + job->p.n_cg) * job->o.event_cap * n);
+        CP(r->event_states, S.ev_st, (size_t)job->o.event_cap * n);
+    }
     const size_t fb = sizeof(double) * (size_t)job->nframe * n;
     if (S.fx) CP(r->frames_x, S.fx, fb);
     if (S.fv) {

@@ -59,9 +59,9 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
         return LDP_ERR_INVALID;
     }
     if (o->mode != LDP_MODE_FIXED_STEPS || p->waiting_time || p->n_cg > LDP_MAX_CG || p->freq_save < 1 ||
-        !(p->timestep > 0.0) || !(p->periodic_length > 0.0)) {
+        !(p->timestep > 0.0) || !(p->periodic_length > 0.0) || p->number_of_previous_steps) {
         set_err(err, errlen, "fixed-step runs only, WAITINGTIME off, at most 16 FPTCG entries, positive "
-                             "TIMESTEP and PERIODICLENGTH, FREQSAVE >= 1");
+                             "TIMESTEP and PERIODICLENGTH, FREQSAVE >= 1, no restart (NUMBEROFPREVIOUSSTEPS 0)");
         return LDP_ERR_UNSUPPORTED;
     }
     int dev = 0;

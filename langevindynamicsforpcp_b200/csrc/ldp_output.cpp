@@ -550,13 +550,22 @@ extern "C" ldp_status ldp_run_inp(ldp_ctx* ctx, const char* path, int model, con
     st = ldp_job_create(ctx, &p, o, &job);
     if (st != LDP_OK) return st;
     std::fprintf(stderr, "Interval = %10zd\n", job->lags.size());
-    st = ldp_submit(ctx, job);
+    // READRESTART: continue the runs saved under INPUTRESTART (Integrate ->
+    // PreIntegrate -> ReadRestartFile, S.h:1344-1348).
+    if (p.read_restart) st = ldp_job_restore(job, p.input_restart);
+    if (st == LDP_OK) st = ldp_submit(ctx, job);
     if (st == LDP_OK) st = ldp_wait(ctx, job);
     if (st == LDP_OK) {
         ldp_timing tm;
         ldp_job_timing_get(job, &tm);
         const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         st = write_outputs_timed(job, outdir, total, tm.integrate_ms * 1e-3, tm.msd_ms * 1e-3, -1.0);
+    }
+    // WRITERESTART: OUTPUTRESTART files after the run (S.h:1513-1517).
+    if (st == LDP_OK && p.write_restart) {
+        const std::string base = (outdir && *outdir) ? std::string(outdir) + "/" + p.output_restart
+                                                     : std::string(p.output_restart);
+        st = ldp_job_save_restart(job, base.c_str());
     }
     ldp_job_destroy(job);
     return st;

@@ -17,8 +17,11 @@ uint64_t effective_steps(const ldp_params& p) {
     return p.number_of_steps;
 }
 
+// Frames of the run, the previous steps of a restart included: the count
+// the runner analyses (CalculateNumberOfFrame(numberOfStep +
+// numberOfStepPrevious, saveFreq), S.h:3220 with S.h:1811).
 int64_t frame_count(const ldp_params& p) {
-    return (int64_t)(p.number_of_steps / p.freq_save + 1);   // CalculateNumberOfFrame, S.h:1811
+    return (int64_t)((p.number_of_steps + p.number_of_previous_steps) / p.freq_save + 1);
 }
 
 static uint64_t to_u64_threshold(double p) {

@@ -211,7 +211,8 @@ uint64_t ldpo_effective_steps(const ldp_params *p) {
 }
 
 int64_t ldpo_nframe(const ldp_params *p) {
-    return (int64_t)(p->number_of_steps / p->freq_save + 1);
+    /* CalculateNumberOfFrame(numberOfStep + numberOfStepPrevious), S.h:3220 */
+    return (int64_t)((p->number_of_steps + p->number_of_previous_steps) / p->freq_save + 1);
 }
 
 static void prepare(const ldp_params *p, ocst *k) {
@@ -362,6 +363,19 @@ typedef struct {
     int64_t cg_well[LDP_MAX_CG];
 } tstate;
 
+/* Appends an event duration to list `list` of trajectory i (the reference's
+ * push_back on its per-lane vectors, S.h:2391, 2447, 2504, 2524, 2580); a
+ * full list flags the trajectory. */
+static void ev_push(const ldpo_cfg *c, ldp_traj_results *out, int64_t n, int64_t i, int list, int64_t cnt, double d,
+                    uint32_t *flags) {
+    if (c->event_cap <= 0) return;
+    if (cnt < c->event_cap) {
+        if (out->events) out->events[((int64_t)list * n + i) * c->event_cap + cnt] = d;
+    } else {
+        *flags |= LDP_FLAG_EVENT_OVERFLOW;
+    }
+}
+
 static int64_t cell_key(const ocst *k, int64_t cell, int lb) {
     return k->dbl ? cell * 2 + lb : cell;
 }
@@ -473,6 +487,7 @@ typedef struct {
 #define SUM(f) out->sums[(int64_t)(f) * n + i]
 
 static void record(const ocst *k, const tstate *t, ldp_traj_results *out, int64_t n, int64_t i, int64_t frame) {
+    if (frame >= k->nframe) return;
     int64_t o = frame * n + i;
     if (out->frames_x) out->frames_x[o] = t->x;
     if (k->write_x) {
@@ -706,8 +721,12 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                         t.fpt_up = 1;
                         if (cnt[LDP_C_FPT] == 0) sum[LDP_S_FIRST_FPT] = now - t.fpt_last;
                         sum[LDP_S_FPT] += now - t.fpt_last;
-                        cnt[LDP_C_FPT]++;
                         double ib = ((double)t.cell == (double)t.init_idx[0]) ? t.init_state[0] : t.init_state[1];
+                        ev_push(c, out, n, i, LDP_E_FPT, cnt[LDP_C_FPT], now - t.fpt_last, &flags);
+                        if (cnt[LDP_C_FPT] < c->event_cap && out->event_states)
+                            out->event_states[i * c->event_cap + cnt[LDP_C_FPT]] =
+                                (uint8_t)((t.state ? 1 : 0) | (ib != 0.0 ? 2 : 0));
+                        cnt[LDP_C_FPT]++;
                         cnt[ib == 0.0 ? LDP_C_INIT0 : LDP_C_INIT1]++;
                         cnt[t.state == 0 ? LDP_C_INST0 : LDP_C_INST1]++;
                     }
@@ -720,6 +739,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                 if (dCell && !t.fpt2_up && t.idx2[0] != t.cell && t.idx2[1] != t.cell) {
                     if (cnt[LDP_C_FPT2] == 0) sum[LDP_S_FIRST_FPT2] = now - t.fpt2_last;
                     sum[LDP_S_FPT2] += now - t.fpt2_last;
+                    ev_push(c, out, n, i, LDP_E_FPT2, cnt[LDP_C_FPT2], now - t.fpt2_last, &flags);
                     cnt[LDP_C_FPT2]++;
                     t.fpt2_last = now;
                     fpt2_set_idx(&t);
@@ -732,6 +752,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                     t.tpt_up = 1;
                     if (cnt[LDP_C_TPT] == 0) sum[LDP_S_FIRST_TPT] = now - t.tpt_last;
                     sum[LDP_S_TPT] += now - t.tpt_last;
+                    ev_push(c, out, n, i, LDP_E_TPT, cnt[LDP_C_TPT], now - t.tpt_last, &flags);
                     cnt[LDP_C_TPT]++;
                 }
                 if (dCell) {
@@ -739,6 +760,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                     else if (t.well != t.tpt2_well) {
                         if (cnt[LDP_C_TPT2] == 0) sum[LDP_S_FIRST_TPT2] = now - t.tpt2_last;
                         sum[LDP_S_TPT2] += now - t.tpt2_last;
+                        ev_push(c, out, n, i, LDP_E_TPT2, cnt[LDP_C_TPT2], now - t.tpt2_last, &flags);
                         cnt[LDP_C_TPT2]++;
                     }
                     t.tpt2_last = now;
@@ -754,6 +776,7 @@ int ldpo_run(const ldp_params *p, const ldpo_cfg *c, ldp_traj_results *out) {
                             t.cg_well[jj] = t.well;
                         } else if (t.well != t.cg_well[jj]) {
                             sum[LDP_S_CG0 + jj] += now - t.cg_last[jj];
+                            ev_push(c, out, n, i, LDP_E_CG0 + jj, cnt[LDP_C_CG0 + jj], now - t.cg_last[jj], &flags);
                             cnt[LDP_C_CG0 + jj]++;
                             t.cg_last[jj] = now;
                             t.cg_well[jj] = t.well;

@@ -27,6 +27,7 @@ typedef struct ldpo_cfg {
     uint32_t job_id;              /* Philox key word 1                     */
     int32_t mode;                 /* ldp_mode                              */
     uint64_t step_cap;            /* FIRST_PASSAGE cap                     */
+    int64_t event_cap;            /* per-event lists kept (0: none)        */
 } ldpo_cfg;
 
 void     ldpo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

@@ -22,7 +22,7 @@ from langevindynamicsforpcp_b200 import _lib as L  # noqa: E402  (struct layouts
 class Cfg(C.Structure):
     _fields_ = [("traj_begin", C.c_int64), ("traj_end", C.c_int64), ("lanes", C.c_int32), ("ranks", C.c_int32),
                 ("table_slots", C.c_int32), ("tick_cap", C.c_int64), ("seed", C.c_uint32), ("job_id", C.c_uint32),
-                ("mode", C.c_int32), ("step_cap", C.c_uint64)]
+                ("mode", C.c_int32), ("step_cap", C.c_uint64), ("event_cap", C.c_int64)]
 
 
 _h = None
@@ -90,13 +90,14 @@ def lags(params):
 
 
 def run(params, seed, lanes=8, ranks=1, traj_begin=0, traj_end=None, table_slots=256, tick_cap=0, job_id=0,
-        mode=0, step_cap=0, frames=True):
+        mode=0, step_cap=0, frames=True, event_cap=0):
     """Runs the oracle; returns the same dict layout as Job.results()."""
     ntot = ranks * params.number_of_runs * lanes
     if traj_end is None:
         traj_end = ntot
     n = traj_end - traj_begin
-    cfg = Cfg(traj_begin, traj_end, lanes, ranks, table_slots, tick_cap, seed & 0xffffffff, job_id, mode, step_cap)
+    cfg = Cfg(traj_begin, traj_end, lanes, ranks, table_slots, tick_cap, seed & 0xffffffff, job_id, mode, step_cap,
+              event_cap)
     nf = int(lib().ldpo_nframe(C.byref(params))) if mode == 0 else 0
     out = {
         "counts": np.zeros((L.NCOUNT, n), np.int64),
@@ -122,6 +123,11 @@ def run(params, seed, lanes=8, ranks=1, traj_begin=0, traj_end=None, table_slots
     if tick_cap > 0:
         out["ticks"] = np.zeros((n, tick_cap), np.int64)
         r.ticks = p(out["ticks"], C.c_int64)
+    if event_cap > 0:
+        out["events"] = np.zeros((L.E_CG0 + params.n_cg, n, event_cap), np.float64)
+        out["event_states"] = np.zeros((n, event_cap), np.uint8)
+        r.events = p(out["events"], C.c_double)
+        r.event_states = p(out["event_states"], C.c_uint8)
     if frames and nf > 0:
         out["frames_x"] = np.zeros((nf, n), np.float64)
         r.frames_x = p(out["frames_x"], C.c_double)

@@ -10,6 +10,9 @@ Outputs (committed; nothing at test time reads the reference tree):
   quick_test_events.npz       the first 2000 per-event FPT / FPT2 / TPT / TPT2
                               times of every lane (in steps), decoded from
                               the four .restart files of that run
+  quick_test_rank0.restart.xz rank 0's .restart file of that run, as the
+                              reference wrote it (xz-compressed): the
+                              fixture of the restart reader and writer
 
 The .restart layout decoded here is the reference's
 LangevinEquationSIMDMultiple::WriteRestartFile (src/langevinDynamicsSingleBarrier.h:1048-1136)
@@ -235,6 +238,10 @@ def main():
         lane_fpt_means=np.array(lane_means),
     )
     print("fpt lanes", lane_counts)
+    import lzma
+    src = os.path.join(ej, "m1.0_t1.00e-05_restart_0_00000_00000.restart")
+    with open(src, "rb") as f, lzma.open(os.path.join(OUT, "quick_test_rank0.restart.xz"), "wb", preset=9) as g:
+        g.write(f.read())
 
 
 if __name__ == "__main__":
