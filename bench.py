@@ -41,10 +41,11 @@ OPS_PER_STEP = 70   # lane instructions per overdamped single-barrier step (algo
 # four steps, two Box-Muller pairs (14 each), update 3, tests 3.
 OPS_PER_STEP_AS_BUILT = (58 + 2 * 14) / 4 + 3 + 3
 NJOBS, NTRAJ, NSTEPS, FREQSAVE = 16, 65536, 300000, 100
-# DRAM bytes per particle-step of the persistent kernel: 0.434 B measured by
-# ncu with frames every 20 steps (8 B per frame = 0.40 B per step of it);
-# scaled to this workload's frame interval.
-DRAM_BYTES_PER_STEP = 0.434 - 8.0 / 20 + 8.0 / FREQSAVE
+# DRAM bytes per particle-step of the persistent kernel: 0.0873 B measured by
+# ncu with frames every 100 steps, of which the frames are 8 B per frame
+# (0.0801 B per step); the rest (0.0072 B: retire records, ring) is kept and
+# the frame part scaled to this workload's frame interval.
+DRAM_BYTES_PER_STEP = 0.0072 + 8.0 / FREQSAVE
 
 
 def workload_params(ldp, job0=0, njobs=NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE):
@@ -311,7 +312,8 @@ def main():
         for j in jobs:
             r = j.results(frames=False, ticks=False)
             lags, msd = j.msd()
-            b_out += r["counts"].nbytes + r["sums"].nbytes + msd.nbytes
+            ncg = j.info.n_cg     # the rows the device holds (the rest are cleared on the host)
+            b_out += 8 * r["counts"].shape[1] * ((ldp._lib.C_CG0 + ncg) + (ldp._lib.S_CG0 + ncg)) + msd.nbytes
             j.close()
         torch.cuda.synchronize()
         if it >= args.warmup:
@@ -341,7 +343,7 @@ def main():
                 "frac": achieved / peak_issue, "traffic": DRAM_BYTES_PER_STEP * psteps,
                 "traffic_scope": "DRAM bytes of the persistent kernel per bench step (all its launches): "
                                  f"{DRAM_BYTES_PER_STEP} B per particle-step from the ncu capture in "
-                                 "profiles/fp32_persistent_kernel__single_over_113664traj_24000steps.md, "
+                                 "profiles/fp32_persistent_kernel__single_over_113664traj_120000steps.md, "
                                  "scaled by particle-steps and frame interval; algorithmic bytes: the frames, 8 B per FREQSAVE steps",
                 "kernel": "fp32_persistent_kernel<single, overdamped>",
                 "ops_per_step": OPS_PER_STEP, "kernel_ms": kms,

@@ -675,8 +675,13 @@ extern "C" ldp_status ldp_job_traj_results(ldp_job* job, ldp_traj_results* r) {
     ldp_status st;
 #define CP(dst, src, bytes) \
     if ((st = copy_d2h(ctx, dst, src, bytes)) != LDP_OK) return st
-    CP(r->counts, S.counts, sizeof(int64_t) * LDP_NCOUNT * n);
-    CP(r->sums, S.sums, sizeof(double) * LDP_NSUM * n);
+    // Rows past the job's FPTCG entries are zero by construction: cleared
+    // on the host instead of copied.
+    const int ncr = LDP_C_CG0 + job->p.n_cg, nsr = LDP_S_CG0 + job->p.n_cg;
+    CP(r->counts, S.counts, sizeof(int64_t) * ncr * n);
+    CP(r->sums, S.sums, sizeof(double) * nsr * n);
+    if (r->counts) std::memset(r->counts + (size_t)ncr * n, 0, sizeof(int64_t) * (LDP_NCOUNT - ncr) * n);
+    if (r->sums) std::memset(r->sums + (size_t)nsr * n, 0, sizeof(double) * (LDP_NSUM - nsr) * n);
     CP(r->state0, S.state0, sizeof(int32_t) * n);
     CP(r->v0, S.v0, sizeof(double) * n);
     CP(r->x_final, S.x, sizeof(double) * n);
