@@ -37,11 +37,6 @@ struct Hist {
         count.assign(nbin, 0.0);
         percent.assign(nbin, 0.0);
     }
-    // HistogramVector: floor index (clsHistogram.cpp:242-255)
-    void add_floor(double v) {
-        const int i = (int)std::floor((v - min) * inv);
-        if (i >= 0 && i < size) count[i] += 1.0;
-    }
     // AddValue: truncation toward zero (clsHistogram.cpp:257-265)
     void add_trunc(double v) {
         const int i = (int)((v - min) * inv);
@@ -128,12 +123,15 @@ double average(const std::vector<double>& v) {
     return s / (double)v.size();
 }
 
-// STATISTICS::RMSD, population standard deviation (src/STATISTICS.cpp:122-134)
+// STATISTICS::RMSD, population standard deviation (src/STATISTICS.cpp:122-134).
+// The squares are accumulated with one rounding each (a fused multiply-add,
+// as the reference's build evaluates `rmsd += d * d`): that is what
+// reproduces the sd lines of its output files to the last digit.
 double rmsd(const std::vector<double>& v) {
     if (v.empty()) return 0.0;
     const double a = average(v);
     double r = 0.0;
-    for (double x : v) r += (x - a) * (x - a);
+    for (double x : v) r = std::fma(x - a, x - a, r);
     return std::sqrt(r / (double)v.size());
 }
 
@@ -336,31 +334,16 @@ static ldp_status write_outputs_timed(ldp_job* job, const char* dir, double t_to
     if (p.fpt) {
         W.dat(base + "_firstPassageTime.dat", means(LDP_C_FPT, LDP_S_FPT));
         W.dat(base + "_firstPassageTime2.dat", means(LDP_C_FPT2, LDP_S_FPT2));
+        // The per-lane histograms of the initial / instantaneous barrier state
+        // lists (S.h:2734-2753) are filled by HISTOGRAM::HistogramVector,
+        // whose loop takes its bounds from the arguments before they are
+        // clamped (src/clsHistogram.cpp:246-255): called with the default
+        // last = -1 it visits no element, so the reference's files always
+        // hold empty histograms.  They are written the same way; the counts
+        // themselves are the LDP_C_INIT0/1 and LDP_C_INST0/1 results.
         Hist hi, hs;
         hi.alloc(0.0, 10.0, 100);
         hs.alloc(0.0, 10.0, 100);
-        std::vector<double> ci_tot(100, 0.0), cs_tot(100, 0.0);
-        for (int rk = 0; rk < R; ++rk) {
-            std::vector<double> ci(100, 0.0), cs(100, 0.0);
-            for (int64_t g = rk * per_rank; g < (rk + 1) * per_rank; ++g) {
-                // per trajectory: histogram of the 0/1 state lists, normalised
-                // to fractions and added into the count (S.h:2734-2753)
-                const double a0 = (double)counts[(size_t)LDP_C_INIT0 * n + g];
-                const double a1 = (double)counts[(size_t)LDP_C_INIT1 * n + g];
-                const double b0 = (double)counts[(size_t)LDP_C_INST0 * n + g];
-                const double b1 = (double)counts[(size_t)LDP_C_INST1 * n + g];
-                const double sa = a0 + a1, sb = b0 + b1;
-                ci[0] += sa != 0.0 ? a0 / sa : 0.0;
-                ci[10] += sa != 0.0 ? a1 / sa : 0.0;
-                cs[0] += sb != 0.0 ? b0 / sb : 0.0;
-                cs[10] += sb != 0.0 ? b1 / sb : 0.0;
-            }
-            for (int i = 0; i < 100; ++i) { ci_tot[i] += ci[i]; cs_tot[i] += cs[i]; }
-        }
-        hi.count = ci_tot;
-        hs.count = cs_tot;
-        hi.normalize();
-        hs.normalize();
         W.stat_log(base + "_firstPassageTime.log", means(LDP_C_FPT, LDP_S_FPT));
         W.stat_log(base + "_firstPassageTime2.log", means(LDP_C_FPT2, LDP_S_FPT2));
         if (FILE* f = W.open(base + "_initialBarrierHeightHistogram.log")) { W.header(f); hi.print(f); std::fclose(f); }
@@ -462,15 +445,11 @@ static ldp_status write_outputs_timed(ldp_job* job, const char* dir, double t_to
         const double Rr = (avg2 - avg * avg) / avg / avg;
         int nbin = 100;
         if (cnt < 1000) nbin = std::max(10, (int)cnt / 100);
+        // Filled by HISTOGRAM::HistogramVector (S.h:3952), which visits no
+        // element (see the barrier histograms above): the reference writes
+        // the bins of the waiting times' range with zero counts.
         Hist h;
         h.alloc(0.0, mx + 0.1, nbin);
-        for (int rk = 0; rk < R; ++rk) {
-            Hist hr;
-            hr.alloc(0.0, mx + 0.1, nbin);
-            for (double x : wl[rk]) hr.add_floor(x);
-            for (int i = 0; i < nbin; ++i) h.count[i] += hr.count[i];
-        }
-        h.normalize();
         if (FILE* f = W.open(base + "_waitingTime.log")) {
             W.header(f);
             std::fprintf(f, "# R      = %13.7f\n", Rr);

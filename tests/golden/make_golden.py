@@ -10,9 +10,13 @@ Outputs (committed; nothing at test time reads the reference tree):
   quick_test_events.npz       the first 2000 per-event FPT / FPT2 / TPT / TPT2
                               times of every lane (in steps), decoded from
                               the four .restart files of that run
-  quick_test_rank0.restart.xz rank 0's .restart file of that run, as the
-                              reference wrote it (xz-compressed): the
-                              fixture of the restart reader and writer
+  quick_test_rank{0..3}.restart.xz
+                              the .restart files of ranks 0-3 of that run,
+                              as the reference wrote them (xz-compressed):
+                              the fixtures of the restart reader and writer
+  quick_test_outputs/         that run's output files (.log, .dat) and one
+                              of its WRITEX trajectory dumps (.log.xz), as
+                              the reference wrote them
 
 The .restart layout decoded here is the reference's
 LangevinEquationSIMDMultiple::WriteRestartFile (src/langevinDynamicsSingleBarrier.h:1048-1136)
@@ -239,8 +243,19 @@ def main():
     )
     print("fpt lanes", lane_counts)
     import lzma
-    src = os.path.join(ej, "m1.0_t1.00e-05_restart_0_00000_00000.restart")
-    with open(src, "rb") as f, lzma.open(os.path.join(OUT, "quick_test_rank0.restart.xz"), "wb", preset=9) as g:
+    for rank in range(4):
+        src = os.path.join(ej, f"m1.0_t1.00e-05_restart_0_{rank:05d}_00000.restart")
+        dst = os.path.join(OUT, f"quick_test_rank{rank}.restart.xz")
+        with open(src, "rb") as f, lzma.open(dst, "wb", preset=9) as g:
+            g.write(f.read())
+    outs = os.path.join(OUT, "quick_test_outputs")
+    os.makedirs(outs, exist_ok=True)
+    for name in sorted(os.listdir(ej)):
+        if name.startswith("m1.0_t1.00e-05_0_") and "trajectory" not in name:
+            shutil.copyfile(os.path.join(ej, name), os.path.join(outs, name))
+    # one WRITEX trajectory dump (trial 0, lane 1, rank 2), xz-compressed
+    name = "m1.0_t1.00e-05_0_trajectory_0000000000_0000000001_0000000002.log"
+    with open(os.path.join(ej, name), "rb") as f, lzma.open(os.path.join(outs, name + ".xz"), "wb", preset=9) as g:
         g.write(f.read())
 
 
