@@ -358,13 +358,7 @@ def main():
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"precision: {NJOBS} single-barrier jobs x {NTRAJ} trajectories, dt 1e-5, "
-                                   f"{NSTEPS} steps, {NSTEPS // FREQSAVE + 1} frames, per-job H in {{2,3,4,5}}, "
-                                   "high 3.6H, flip rate logU[1e-2,1e2]",
-                       "trajectories": NJOBS * NTRAJ * world, "steps_per_trajectory": NSTEPS,
-                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before each step; "
-                                                                 "frames 25 GB per step",
-                       "fp32_shape": shape_used, "tuned": bool(shape)},
+            "config": dict(workload_config(world), fp32_shape=shape_used, tuned=bool(shape)),
             "fp64_plain": {"value": fp64_value, "unit": "particle-steps/s",
                            "sample": f"job 0 alone ({NTRAJ} trajectories x {NSTEPS} steps)"},
             "fp32_over_fp64": value / world / fp64_value,
@@ -382,6 +376,17 @@ def main():
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def workload_config(world):
+    """The workload both arms measure (the reference arm on a bounded sample
+    of it, described in its cpu_baseline)."""
+    return {"workload": f"precision: {NJOBS} single-barrier jobs x {NTRAJ} trajectories, dt 1e-5, "
+                        f"{NSTEPS} steps, {NSTEPS // FREQSAVE + 1} frames, per-job H in {{2,3,4,5}}, "
+                        "high 3.6H, flip rate logU[1e-2,1e2]",
+            "trajectories": NJOBS * NTRAJ * world, "steps_per_trajectory": NSTEPS,
+            "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MB write) before each step; frames 25 GB per step"}
 
 
 def C_sizeof_params():
@@ -405,7 +410,7 @@ def bench_reference(args, rank, world):
     line = {"impl": "reference", "metric": "particle-steps/s, FP32 batched (vs FP64 plain), 1xB200",
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "precision: job 0 of the 16-job workload, bounded sample per step"},
+            "config": workload_config(world),
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": kind,
                              "sample": r["sample"]},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
