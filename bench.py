@@ -215,11 +215,8 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from langevindynamicsforpcp_b200.replicas import Replicas
+    rep = Replicas("nccl", timeout_s=120)
 
     import langevindynamicsforpcp_b200 as ldp
     from langevindynamicsforpcp_b200 import _tune
@@ -239,12 +236,11 @@ def main():
     ctx = ldp.Context(local)
     shape = _tune.apply_tuned(ctx, "single_over")
     params = workload_params(ldp, 0, NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE)
-    job_id0 = rank * 1000   # replicas integrate different trajectories
+    job_id0 = rep.job_id_base   # replicas integrate different trajectories
     psteps = NJOBS * NTRAJ * NSTEPS
 
     def barrier():
-        if dist:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
 
     # ---- FP32 batched, device-resident timing ----
@@ -274,14 +270,7 @@ def main():
             for j in jobs:
                 j.close()
     clocks = clk.summary()
-    step_ms = max(times) if world == 1 else None
-    my_ms = sum(times) / len(times)
-    if dist:
-        tt = torch.tensor([my_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_ms = tt.item()
-    else:
-        step_ms = my_ms
+    step_ms = rep.max_over_ranks(sum(times) / len(times))
     value = psteps * world / (step_ms * 1e-3)
     shape_used = _tune.get_fp32_shape(ctx)
 
@@ -319,11 +308,7 @@ def main():
         if it >= args.warmup:
             e2e_t.append(time.perf_counter() - t0)
             h2d, d2h = b_in, b_out
-    e2e_s = sum(e2e_t) / len(e2e_t)
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = tt.item()
+    e2e_s = rep.max_over_ranks(sum(e2e_t) / len(e2e_t))
     e2e_value = psteps * world / e2e_s
 
     # ---- roofline of the persistent kernel (issue-bound) ----
@@ -374,8 +359,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     ctx.close()
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def workload_config(world):
