@@ -768,12 +768,13 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
                 rv = fmaf(c3, rv, nz);
                 xp = fmaf(rv, c2, xp);
             }
-            --left;
-            if (__builtin_expect(!(xp > lo && xp < hi) || left == 0, 0)) {
+            // left counts from the quad's start: the countdown ends at this
+            // sub-step when it equals h + 1 (one decrement per quad)
+            if (__builtin_expect(!(xp > lo && xp < hi) || left == h + 1, 0)) {
                 sm.xp[t] = xp;
                 sm.rv[t] = rv;
                 sm.F[t] = F;
-                sm.left[t] = left;
+                sm.left[t] = left - (h + 1);
                 sm.lo[t] = lo;
                 sm.hi[t] = hi;
                 general_step<DBL, OVER>(q.jobs, &S, &sm, t, slot, 4 * j + 1 + h);
@@ -781,11 +782,12 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
                 F = sm.F[t];
                 lo = sm.lo[t];
                 hi = sm.hi[t];
-                left = sm.left[t];
+                left = sm.left[t] + (h + 1);
                 job = sm.job[t];
             }
             if (!OVER) rv = fmaf(F, c1, rv);
         }
+        left -= 4;
         ++j;
     }
 
