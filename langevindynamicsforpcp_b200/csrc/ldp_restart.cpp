@@ -754,6 +754,17 @@ extern "C" ldp_status ldp_job_restore(ldp_job* job, const char* base) {
                 return LDP_ERR_RESTART;
             }
             for (const Lane& a : f.lanes) {
+                // Values that become integers on the device must be finite
+                // and in range (a damaged file must not reach the casts).
+                const double idx_max = 0x1p52;
+                const double ints[] = {a.cell, a.well, a.lb, a.wt_prev, a.state, a.state0, a.sc[0], a.sc[1]};
+                bool ok = std::isfinite(a.x) && std::isfinite(a.v);
+                for (double d : ints) ok = ok && std::isfinite(d) && std::fabs(d) < idx_max;
+                if (!ok) {
+                    ldp_set_error(ctx, "restart file corrupted: non-finite or out-of-range lane state (%s)",
+                                  path.c_str());
+                    return LDP_ERR_RESTART;
+                }
                 need_ev = std::max({need_ev, a.fpt.size(), a.fpt2.size(), a.tpt.size(), a.tpt2.size()});
                 for (const auto& c : a.cg) need_ev = std::max(need_ev, c.list.size());
                 need_ticks = std::max(need_ticks, a.ticks.size());

@@ -149,7 +149,17 @@ def test_restart_errors(ctx, tmp_path):
     base = str(tmp_path / "e")
     with ldp.Job(ctx, quick(300_000), lanes=8, event_cap=CAP) as job:
         job.run()
+        x0 = job.results(frames=False)["x_final"][0]
         job.save_restart(base)
+    # a damaged file: lane 0's position replaced by NaN
+    data = open(base + "_00000_00000.restart", "rb").read()
+    at = data.find(struct.pack("<d", x0))
+    assert at > 0
+    bad = str(tmp_path / "bad")
+    open(bad + "_00000_00000.restart", "wb").write(data[:at] + struct.pack("<d", float("nan")) + data[at + 8:])
+    with ldp.Job(ctx, quick(300_000, number_of_previous_steps=300_000), lanes=8, event_cap=CAP) as job:
+        with pytest.raises(ldp.LdpError, match="corrupted"):
+            job.restore(bad)
     # step count must match NUMBEROFPREVIOUSSTEPS
     with ldp.Job(ctx, quick(300_000, number_of_previous_steps=200_000), lanes=8, event_cap=CAP) as job:
         with pytest.raises(ldp.LdpError, match="NUMBEROFPREVIOUSSTEPS"):
