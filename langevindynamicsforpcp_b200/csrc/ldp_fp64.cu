@@ -282,6 +282,8 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
     uint32_t flags = 0;
     uint64_t s = s_begin;
     const uint64_t fs = k.freq_save;
+    // Next frame step (a multiple of FREQSAVE), so that no step divides.
+    uint64_t nxf = (s_begin + fs - 1) / fs * fs;
     // One Philox block serves steps 4a+1 .. 4a+4: words 0,1 the first
     // Gaussian pair, words 2,3 (kept) the second.
     double za = 0, zb = 0;
@@ -473,7 +475,10 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
                 }
             }
         }
-        if (!k.fp_mode && (s % fs) == 0) record(k, st, t, i, (int64_t)(s / fs));
+        if (!k.fp_mode && s == nxf) {
+            record(k, st, t, i, (int64_t)(s / fs));
+            nxf += fs;
+        }
         if (t.bits & B_DONE) { ++s; break; }
     }
     // s is the first step not integrated.
