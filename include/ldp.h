@@ -344,6 +344,15 @@ ldp_status  ldp_job_traj_results(ldp_job *job, ldp_traj_results *out);
  * divided by nrun, src/langevinDynamicsSingleBarrier.h:24-45, 3452-3461,
  * 3893-3912); lags in frames. */
 ldp_status  ldp_job_msd(ldp_job *job, int64_t *lags, double *msd, int64_t nlag);
+/* Per-trajectory mean event times (time units) of each event list, the
+ * reference's getters GetFirstPassageTimeAverage{,2},
+ * GetTransitionPathTimeAverage{,2} and GetFirstPassageTimeCGAverage2
+ * (src/langevinDynamicsSingleBarrier.h:2722-2763): sum / count of the
+ * list, 0 for a list without events (STATISTICS::AVERAGE,
+ * src/STATISTICS.cpp:100-106); laid out [LDP_E_CG0 + n_cg][ntraj] in
+ * ldp_event_list order.  Computed on the device: only the means are
+ * copied. */
+ldp_status  ldp_job_traj_means(ldp_job *job, double *means);
 /* Per-trajectory MSD before the sum over trajectories (the reference's msd0
  * of one lane, S.h:3454-3455), [nlag][ntraj]. */
 ldp_status  ldp_job_msd_traj(ldp_job *job, double *msd0);

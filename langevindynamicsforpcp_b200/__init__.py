@@ -199,6 +199,14 @@ class Job:
         _check(L.lib().ldp_job_msd(self.handle, _ptr(lags, C.c_int64), _ptr(msd, C.c_double), i.nlag), self.ctx)
         return lags, msd
 
+    def means(self) -> np.ndarray:
+        """Per-trajectory mean event times [list][traj] (ldp_job_traj_means):
+        the reference's per-lane averages, computed on the device."""
+        i = self.info
+        m = np.zeros((L.E_CG0 + i.n_cg, i.ntraj), np.float64)
+        _check(L.lib().ldp_job_traj_means(self.handle, _ptr(m, C.c_double)), self.ctx)
+        return m
+
     def msd_traj(self) -> np.ndarray:
         i = self.info
         m = np.zeros((i.nlag, i.ntraj), np.float64)

@@ -150,6 +150,7 @@ SIGNATURES = {
     "ldp_job_traj_results": (C.c_int, [C.c_void_p, C.POINTER(TrajResults)]),
     "ldp_job_msd": (C.c_int, [C.c_void_p, _I64P, _DP, C.c_int64]),
     "ldp_job_msd_traj": (C.c_int, [C.c_void_p, _DP]),
+    "ldp_job_traj_means": (C.c_int, [C.c_void_p, _DP]),
     "ldp_job_write_outputs": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ldp_run_inp": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(JobOpts), C.c_char_p]),
     "ldp_server_opts_default": (None, [C.POINTER(ServerOpts)]),

@@ -47,6 +47,7 @@ struct ldp_job {
     double* d_msd = nullptr;
     int64_t* d_lags = nullptr;
     void* d_aux = nullptr;   // 4 KiB of job-private device scratch
+    double* d_means = nullptr;   // per-trajectory mean event times [list][ntraj]
     int64_t* d_ssum = nullptr;   // FP32 batched: event durations in steps [LDP_NSUM][ntraj]
     int32_t* d_i32b = nullptr;   // FP32 batched: 32-bit statistics state
     int fp32_type = -1;          // FP32 batched: queue (dbl*2 + over) the job is in

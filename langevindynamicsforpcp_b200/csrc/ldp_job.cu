@@ -23,6 +23,7 @@
 namespace ldp {
 int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
                double* msd0, double* msd_sum, void* stream);
+int launch_traj_means(const int64_t* counts, const double* sums, double* means, int64_t n, int ncg, void* stream);
 }  // namespace ldp
 
 using namespace ldp;
@@ -306,6 +307,7 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     const size_t o_msd = take(sizeof(double) * (size_t)std::max<int64_t>(nlag, 1));
     const size_t o_lag = take(sizeof(int64_t) * (size_t)std::max<int64_t>(nlag, 1));
     const size_t o_aux = take(4096);
+    const size_t o_mean = take(sizeof(double) * (LDP_E_CG0 + p->n_cg) * n);
     // FP32 batched extras: integer event-duration sums and 32-bit cell indices.
     const size_t o_ssum = take(f32 ? sizeof(int64_t) * LDP_NSUM * n : 0);
     const size_t o_i32b = take(f32 ? sizeof(int32_t) * (5 + ncg_rows) * n : 0);
@@ -351,6 +353,7 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     job->d_msd = (double*)(a + o_msd);
     job->d_lags = (int64_t*)(a + o_lag);
     job->d_aux = (void*)(a + o_aux);
+    job->d_means = (double*)(a + o_mean);
     job->d_ssum = f32 ? (int64_t*)(a + o_ssum) : nullptr;
     job->d_i32b = f32 ? (int32_t*)(a + o_i32b) : nullptr;
     if (nlag > 0)
@@ -726,6 +729,28 @@ extern "C" ldp_status ldp_job_msd(ldp_job* job, int64_t* lags, double* msd, int6
         const double nrun = (double)job->ntraj;
         for (int64_t i = 0; i < nl; ++i) msd[i] = sum[i] / nrun;
     }
+    return LDP_OK;
+}
+
+// Per-trajectory mean event times, computed on the device so that only
+// the means cross to the host: [LDP_E_CG0 + n_cg][ntraj].
+extern "C" ldp_status ldp_job_traj_means(ldp_job* job, double* means) {
+    if (!job || !means) return LDP_ERR_INVALID;
+    if (!job->done) {
+        ldp_status st = ldp_wait(job->ctx, job);
+        if (st != LDP_OK) return st;
+    }
+    ldp_ctx* ctx = job->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int e = launch_traj_means(job->st.counts, job->st.sums, job->d_means, job->ntraj, job->p.n_cg, s);
+    if (e) {
+        ldp_set_error(ctx, "means launch failed: %s", cudaGetErrorString((cudaError_t)e));
+        return LDP_ERR_DEVICE;
+    }
+    const size_t bytes = sizeof(double) * (LDP_E_CG0 + job->p.n_cg) * (size_t)job->ntraj;
+    CUDA_OR_FAIL(ctx, cudaMemcpyAsync(means, job->d_means, bytes, cudaMemcpyDeviceToHost, s));
+    CUDA_OR_FAIL(ctx, cudaStreamSynchronize(s));
     return LDP_OK;
 }
 

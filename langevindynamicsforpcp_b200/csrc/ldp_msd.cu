@@ -23,6 +23,7 @@
 // fixed shared-memory tree), so the result does not depend on scheduling.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include "../../include/ldp.h"
 
 namespace ldp {
 
@@ -134,6 +135,34 @@ __global__ void __launch_bounds__(BLOCK) msd_reduce_kernel(const double* __restr
         __syncthreads();
     }
     if (threadIdx.x == 0) out[ii] = ss[0] - sc[0];
+}
+
+// Per-trajectory mean event times, [list][traj]: the reference's
+// STATISTICS::AVERAGE of each per-lane event list (GetFirstPassageTimeAverage
+// {,2}, GetTransitionPathTimeAverage{,2}, GetFirstPassageTimeCGAverage2,
+// S.h:2722-2763; src/STATISTICS.cpp:100-106): sum / count, 0 for no event.
+// List L reads count field L and sum field L for L < 4 (FPT, FPT2, TPT,
+// TPT2) and the FPTCG fields for the rest.
+__global__ void traj_means_kernel(const int64_t* __restrict__ counts, const double* __restrict__ sums,
+                                  double* __restrict__ means, int64_t n, int nlists) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)nlists * n) return;
+    const int L = (int)(idx / n);
+    const int64_t i = idx - (int64_t)L * n;
+    const int cf = L < LDP_E_CG0 ? L : LDP_C_CG0 + (L - LDP_E_CG0);
+    const int sf = L < LDP_E_CG0 ? L : LDP_S_CG0 + (L - LDP_E_CG0);
+    const int64_t c = counts[(int64_t)cf * n + i];
+    means[idx] = c ? sums[(int64_t)sf * n + i] / (double)c : 0.0;
+}
+
+int launch_traj_means(const int64_t* counts, const double* sums, double* means, int64_t n, int ncg, void* stream) {
+    const int nlists = LDP_E_CG0 + ncg;
+    const int64_t total = (int64_t)nlists * n;
+    if (total == 0) return 0;
+    const int block = 256;
+    traj_means_kernel<<<(unsigned)((total + block - 1) / block), block, 0, (cudaStream_t)stream>>>(counts, sums, means,
+                                                                                               n, nlists);
+    return (int)cudaGetLastError();
 }
 
 int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
