@@ -20,7 +20,7 @@
 
 namespace ldp {
 int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
-               double* msd0, double* msd_sum, void* stream);
+               double* msd0, double* msd_sum, void* stream, bool f32);
 
 struct Fp32Queue {
     bool ready = false;
@@ -373,7 +373,7 @@ int fp32_finalize(ldp_job* job, cudaStream_t stream) {
     ++job->launches;
     if (job->o.mode == LDP_MODE_FIXED_STEPS && !job->lags.empty()) {
         e = launch_msd(job->st.fx, job->nframe, job->ntraj, job->d_lags, (int64_t)job->lags.size(), job->d_msd0,
-                       job->d_msd, st);
+                       job->d_msd, st, true);
         if (e) return e;
         job->launches += 2;
     }

@@ -22,7 +22,7 @@
 
 namespace ldp {
 int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
-               double* msd0, double* msd_sum, void* stream);
+               double* msd0, double* msd_sum, void* stream, bool f32);
 int launch_traj_means(const int64_t* counts, const double* sums, double* means, int64_t n, int ncg, void* stream);
 }  // namespace ldp
 
@@ -522,7 +522,7 @@ extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
     }
     if (job->o.mode == LDP_MODE_FIXED_STEPS && !job->lags.empty()) {
         int e = launch_msd(job->st.fx, job->nframe, job->ntraj, job->d_lags, (int64_t)job->lags.size(), job->d_msd0,
-                           job->d_msd, s);
+                           job->d_msd, s, false);
         if (e) {
             ldp_set_error(ctx, "MSD launch failed: %s", cudaGetErrorString((cudaError_t)e));
             return LDP_ERR_DEVICE;

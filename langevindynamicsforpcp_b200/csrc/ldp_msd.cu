@@ -18,6 +18,13 @@
 // msd_traj_kernel is the same computation from global memory, used only when
 // one trajectory's frames do not fit in shared memory.
 //
+// msd_smem_f32_kernel: the same for jobs of the FP32 batched path, in FP32:
+// a trajectory's frames are staged as offsets from its first frame, rounded
+// to FP32 (an error of at most 2^-24 of the offset), and the squares are
+// summed in FP32 (32-way interleaved partials of ~nframe/32 terms each).  Half the shared-memory bytes per term,
+// which bound the FP64 kernel.  The FP64 plain path keeps the FP64 kernel
+// (bit-identical to the oracle).
+//
 // msd_reduce_kernel: one block per lag sums msd0 over trajectories with
 // Kahan compensation in a fixed order (per-thread strided partials, then a
 // fixed shared-memory tree), so the result does not depend on scheduling.
@@ -82,6 +89,60 @@ __global__ void __launch_bounds__(kMsdBlock) msd_smem_kernel(const double* __res
             for (int h = 16; h >= 1; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
             const int i = g0 + r;
             if (lane == 0 && i < nlag) msd0[(int64_t)i * ntraj + t0 + j] = cnt[r] > 0 ? v / (double)cnt[r] : 0.0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMsdBlock) msd_smem_f32_kernel(const double* __restrict__ frames, int nframe,
+                                                                 int64_t ntraj, int G,
+                                                                 const int64_t* __restrict__ lags, int nlag,
+                                                                 double* __restrict__ msd0) {
+    extern __shared__ float fs32[];   // [G][nframe]
+    const int64_t t0 = (int64_t)blockIdx.x * G;
+    const int gh = (int)((ntraj - t0) < G ? (ntraj - t0) : G);
+    const int total = nframe * G;
+    for (int e = threadIdx.x; e < total; e += kMsdBlock) {
+        const int k = e / G;
+        const int j = e - k * G;
+        fs32[j * nframe + k] = (j < gh) ? (float)(frames[(int64_t)k * ntraj + t0 + j] - frames[t0 + j]) : 0.0f;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ngroup = (nlag + kMsdLags - 1) / kMsdLags;
+    const int items = gh * ngroup;
+    for (int it = warp; it < items; it += kMsdBlock / 32) {
+        const int j = it / ngroup;
+        const int g0 = (it - j * ngroup) * kMsdLags;
+        const float* x = fs32 + j * nframe;
+        int lag[kMsdLags], cnt[kMsdLags];
+        float acc[kMsdLags];
+        int kmax = 0;
+#pragma unroll
+        for (int r = 0; r < kMsdLags; ++r) {
+            const int i = g0 + r;
+            lag[r] = (i < nlag) ? (int)lags[i] : 0;
+            cnt[r] = (i < nlag) ? nframe - lag[r] : 0;
+            if (cnt[r] < 0) cnt[r] = 0;
+            kmax = cnt[r] > kmax ? cnt[r] : kmax;
+            acc[r] = 0.0f;
+        }
+        for (int k = lane; k < kmax; k += 32) {
+            const float xk = x[k];
+#pragma unroll
+            for (int r = 0; r < kMsdLags; ++r) {
+                if (k < cnt[r]) {
+                    const float d = x[k + lag[r]] - xk;
+                    acc[r] = fmaf(d, d, acc[r]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kMsdLags; ++r) {
+            float v = acc[r];
+#pragma unroll
+            for (int h = 16; h >= 1; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
+            const int i = g0 + r;
+            if (lane == 0 && i < nlag) msd0[(int64_t)i * ntraj + t0 + j] = cnt[r] > 0 ? (double)v / (double)cnt[r] : 0.0;
         }
     }
 }
@@ -166,18 +227,26 @@ int launch_traj_means(const int64_t* counts, const double* sums, double* means, 
 }
 
 int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
-               double* msd0, double* msd_sum, void* stream) {
+               double* msd0, double* msd_sum, void* stream, bool f32) {
     cudaStream_t s = (cudaStream_t)stream;
-    const int64_t per_traj = nframe * (int64_t)sizeof(double);
+    const int64_t per_traj = nframe * (int64_t)(f32 ? sizeof(float) : sizeof(double));
     int G = (int)(kMsdSmemBytes / (per_traj > 0 ? per_traj : 1));
     if (G > 32) G = 32;
     cudaError_t e;
     if (G >= 1 && nframe < (1 << 30) && nlag < (1 << 30)) {
         const size_t smem = (size_t)G * (size_t)per_traj;
-        e = cudaFuncSetAttribute(msd_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return (int)e;
         const int64_t nblk = (ntraj + G - 1) / G;
-        msd_smem_kernel<<<(unsigned)nblk, kMsdBlock, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag, msd0);
+        if (f32) {
+            e = cudaFuncSetAttribute(msd_smem_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return (int)e;
+            msd_smem_f32_kernel<<<(unsigned)nblk, kMsdBlock, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag,
+                                                                       msd0);
+        } else {
+            e = cudaFuncSetAttribute(msd_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return (int)e;
+            msd_smem_kernel<<<(unsigned)nblk, kMsdBlock, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag,
+                                                                   msd0);
+        }
     } else {
         const int block = 256;
         dim3 grid((unsigned)((ntraj + 7) / 8), (unsigned)nlag);

@@ -161,6 +161,25 @@ def test_fp32_statistics_agree_with_fp64(ctx):
     np.testing.assert_allclose(b["msd"][ok], a["msd"][ok], rtol=0.02)
 
 
+def test_fp32_msd_matches_an_fp64_msd_of_its_own_frames(ctx):
+    # The FP32 path's MSD kernel stages each trajectory's frames as FP32
+    # offsets from its first frame and sums the squares in FP32.  Against an
+    # FP64 brute-force MSD of the same saved frames, every per-trajectory
+    # value is within 1e-5 relative (staging rounding ~1e-7, FP32 partial
+    # sums of <= 94 terms ~1e-6).
+    p = quick(steps=120_000, freq=40)
+    with ldp.Job(ctx, p, precision=ldp.PREC_FP32_BATCHED, lanes=500) as job:
+        job.run()
+        fx = job.results()["frames_x"]
+        lags, msd = job.msd()
+        m0 = job.msd_traj()
+    assert fx.shape == (3001, 500) and len(lags) > 20
+    nf = fx.shape[0]
+    want = np.stack([((fx[L:] - fx[:nf - L]) ** 2).mean(0) for L in lags])
+    np.testing.assert_allclose(m0, want, rtol=1e-5)
+    np.testing.assert_allclose(msd, want.mean(1), rtol=1e-5)
+
+
 def test_fp32_first_passage_distribution_matches_fp64(ctx):
     # First bottom-to-other-bottom passage of 16384 trajectories in both
     # precisions: two-sample KS p > 0.01 and means within 3 standard errors.
