@@ -21,9 +21,12 @@
 // msd_smem_f32_kernel: the same for jobs of the FP32 batched path, in FP32:
 // a trajectory's frames are staged as offsets from its first frame, rounded
 // to FP32 (an error of at most 2^-24 of the offset), and the squares are
-// summed in FP32 (32-way interleaved partials of ~nframe/32 terms each).  Half the shared-memory bytes per term,
-// which bound the FP64 kernel.  The FP64 plain path keeps the FP64 kernel
-// (bit-identical to the oracle).
+// summed in FP32 (32-way interleaved partials of ~nframe/32 terms each).
+// Half the shared-memory bytes per term, which bound the FP64 kernel; with
+// 8 lags per item, a loop without per-term tests over the origins all of
+// them have, and four blocks per SM (54 KiB each) to hide the shared-load
+// latency.  The FP64 plain path keeps the FP64 kernel (bit-identical to
+// the oracle).
 //
 // msd_reduce_kernel: one block per lag sums msd0 over trajectories with
 // Kahan compensation in a fixed order (per-thread strided partials, then a
@@ -37,6 +40,8 @@ namespace ldp {
 constexpr int kMsdSmemBytes = 100 * 1024;   // two blocks per SM
 constexpr int kMsdBlock = 256;
 constexpr int kMsdLags = 4;                  // lags per work item (x[k] reuse)
+constexpr int kMsdF32SmemBytes = 54 * 1024;  // FP32 kernel: four blocks per SM
+constexpr int kMsdF32Lags = 8;
 
 __global__ void __launch_bounds__(kMsdBlock) msd_smem_kernel(const double* __restrict__ frames, int nframe,
                                                              int64_t ntraj, int G, const int64_t* __restrict__ lags,
@@ -93,10 +98,10 @@ __global__ void __launch_bounds__(kMsdBlock) msd_smem_kernel(const double* __res
     }
 }
 
-__global__ void __launch_bounds__(kMsdBlock) msd_smem_f32_kernel(const double* __restrict__ frames, int nframe,
-                                                                 int64_t ntraj, int G,
-                                                                 const int64_t* __restrict__ lags, int nlag,
-                                                                 double* __restrict__ msd0) {
+__global__ void __launch_bounds__(kMsdBlock, 4) msd_smem_f32_kernel(const double* __restrict__ frames, int nframe,
+                                                                    int64_t ntraj, int G,
+                                                                    const int64_t* __restrict__ lags, int nlag,
+                                                                    double* __restrict__ msd0) {
     extern __shared__ float fs32[];   // [G][nframe]
     const int64_t t0 = (int64_t)blockIdx.x * G;
     const int gh = (int)((ntraj - t0) < G ? (ntraj - t0) : G);
@@ -108,28 +113,42 @@ __global__ void __launch_bounds__(kMsdBlock) msd_smem_f32_kernel(const double* _
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ngroup = (nlag + kMsdLags - 1) / kMsdLags;
+    const int ngroup = (nlag + kMsdF32Lags - 1) / kMsdF32Lags;
     const int items = gh * ngroup;
     for (int it = warp; it < items; it += kMsdBlock / 32) {
         const int j = it / ngroup;
-        const int g0 = (it - j * ngroup) * kMsdLags;
+        const int g0 = (it - j * ngroup) * kMsdF32Lags;
         const float* x = fs32 + j * nframe;
-        int lag[kMsdLags], cnt[kMsdLags];
-        float acc[kMsdLags];
-        int kmax = 0;
+        int lag[kMsdF32Lags], cnt[kMsdF32Lags];
+        float acc[kMsdF32Lags];
+        // Slots past the last lag repeat the group's first lag (results not
+        // written), so that kmin is the shortest origin count of real lags.
+        const int lag0 = (int)lags[g0];
+        int kmin = 1 << 30, kmax = 0;
 #pragma unroll
-        for (int r = 0; r < kMsdLags; ++r) {
+        for (int r = 0; r < kMsdF32Lags; ++r) {
             const int i = g0 + r;
-            lag[r] = (i < nlag) ? (int)lags[i] : 0;
-            cnt[r] = (i < nlag) ? nframe - lag[r] : 0;
+            lag[r] = (i < nlag) ? (int)lags[i] : lag0;
+            cnt[r] = nframe - lag[r];
             if (cnt[r] < 0) cnt[r] = 0;
+            kmin = cnt[r] < kmin ? cnt[r] : kmin;
             kmax = cnt[r] > kmax ? cnt[r] : kmax;
             acc[r] = 0.0f;
         }
-        for (int k = lane; k < kmax; k += 32) {
+        // Origins every lag of the item has: no per-term test.
+        int k = lane;
+        for (; k < kmin; k += 32) {
             const float xk = x[k];
 #pragma unroll
-            for (int r = 0; r < kMsdLags; ++r) {
+            for (int r = 0; r < kMsdF32Lags; ++r) {
+                const float d = x[k + lag[r]] - xk;
+                acc[r] = fmaf(d, d, acc[r]);
+            }
+        }
+        for (; k < kmax; k += 32) {
+            const float xk = x[k];
+#pragma unroll
+            for (int r = 0; r < kMsdF32Lags; ++r) {
                 if (k < cnt[r]) {
                     const float d = x[k + lag[r]] - xk;
                     acc[r] = fmaf(d, d, acc[r]);
@@ -137,7 +156,7 @@ __global__ void __launch_bounds__(kMsdBlock) msd_smem_f32_kernel(const double* _
             }
         }
 #pragma unroll
-        for (int r = 0; r < kMsdLags; ++r) {
+        for (int r = 0; r < kMsdF32Lags; ++r) {
             float v = acc[r];
 #pragma unroll
             for (int h = 16; h >= 1; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
@@ -230,7 +249,8 @@ int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_
                double* msd0, double* msd_sum, void* stream, bool f32) {
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t per_traj = nframe * (int64_t)(f32 ? sizeof(float) : sizeof(double));
-    int G = (int)(kMsdSmemBytes / (per_traj > 0 ? per_traj : 1));
+    int G = (int)((f32 ? kMsdF32SmemBytes : kMsdSmemBytes) / (per_traj > 0 ? per_traj : 1));
+    if (f32 && G < 1 && per_traj <= kMsdSmemBytes) G = 1;
     if (G > 32) G = 32;
     cudaError_t e;
     if (G >= 1 && nframe < (1 << 30) && nlag < (1 << 30)) {
