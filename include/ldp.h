@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define LDP_ABI_VERSION 1
+#define LDP_ABI_VERSION 2
 #define LDP_MAX_CG 16      /* FPTCG entries accepted per job              */
 #define LDP_PATH_MAX 512   /* OUTPUTBASE / restart base name buffer sizes */
 
@@ -310,15 +310,24 @@ typedef enum {
     LDP_SRV_QUEUED = 0, LDP_SRV_RUNNING = 1, LDP_SRV_FINISHING = 2, LDP_SRV_DONE = 3, LDP_SRV_FAILED = 4
 } ldp_server_state;
 typedef struct ldp_server_opts {
-    int64_t hbm_budget;     /* bytes of job arenas resident at once (0: 80% of free memory) */
+    int64_t hbm_budget;     /* bytes of job arenas resident at once (0: 80% of free memory,
+                               counting what the device's memory pool holds unused)        */
     int64_t pair_budget;    /* step pairs per slot per persistent launch (0: 1024)           */
     int32_t max_inflight;   /* persistent launches in flight per model type (1..16)         */
-    int32_t pad;
+    int32_t region;         /* 1 (default): allocate the budget once, at creation, as one
+                               device region that admitted jobs' arenas are placed in (no
+                               device allocation per job); 0: each arena from the device's
+                               stream-ordered pool                                          */
 } ldp_server_opts;
 typedef struct ldp_server_info {
     int64_t queued, running, finishing, done;
     int64_t hbm_in_use, hbm_budget;
     int64_t launches;
+    int64_t steps;            /* ldp_server_step calls                                      */
+    /* Host seconds spent in each phase of ldp_server_step (admission
+     * bookkeeping and arena allocation, registration, publication, launches,
+     * completion, finished jobs): total and longest single call.          */
+    double phase_s[6], phase_max_s[6];
 } ldp_server_info;
 void        ldp_server_opts_default(ldp_server_opts *o);
 ldp_status  ldp_server_create(ldp_ctx *ctx, const ldp_server_opts *o, ldp_server **out);

@@ -102,12 +102,13 @@ class RestartSummary(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget", C.c_int64), ("pair_budget", C.c_int64), ("max_inflight", C.c_int32),
-                ("pad", C.c_int32)]
+                ("region", C.c_int32)]
 
 
 class ServerInfo(C.Structure):
     _fields_ = [("queued", C.c_int64), ("running", C.c_int64), ("finishing", C.c_int64), ("done", C.c_int64),
-                ("hbm_in_use", C.c_int64), ("hbm_budget", C.c_int64), ("launches", C.c_int64)]
+                ("hbm_in_use", C.c_int64), ("hbm_budget", C.c_int64), ("launches", C.c_int64), ("steps", C.c_int64),
+                ("phase_s", C.c_double * 6), ("phase_max_s", C.c_double * 6)]
 
 
 SRV_QUEUED, SRV_RUNNING, SRV_FINISHING, SRV_DONE, SRV_FAILED = range(5)
@@ -181,6 +182,9 @@ class LdpError(RuntimeError):
         super().__init__(f"{STATUS.get(status, status)}: {msg}" if msg else STATUS.get(status, str(status)))
 
 
+ABI_VERSION = 2   # LDP_ABI_VERSION of include/ldp.h that these structures mirror
+
+
 def lib() -> C.CDLL:
     """Loads libldp.so once; raises if it was not built."""
     global _lib
@@ -193,5 +197,8 @@ def lib() -> C.CDLL:
             f = getattr(h, name)
             f.restype = res
             f.argtypes = args
+        if h.ldp_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {h.ldp_abi_version()}, these bindings expect "
+                               f"{ABI_VERSION}: rebuild it with `make -C {HERE}`")
         _lib = h
     return _lib

@@ -42,6 +42,7 @@ struct ldp_job {
     std::vector<int64_t> lags;
     void* arena = nullptr;
     size_t arena_bytes = 0;
+    bool arena_owned = false;    // allocated by the job (else placed by its owner)
     ldp::TrajState st{};
     double* d_msd0 = nullptr;
     double* d_msd = nullptr;
@@ -93,3 +94,6 @@ std::vector<int64_t> ldp_lag_grid(const ldp_params& p);
 // (size, or allocation): the serving loop admits jobs by footprint itself.
 ldp_status ldp_job_create_unchecked(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out);
 size_t ldp_job_arena(ldp_job* job, bool alloc);
+// Lays the job's arena out at `base` (ldp_job_arena(job, false) bytes owned
+// by the caller, who keeps them until the job is destroyed) and zeroes it.
+size_t ldp_job_arena_at(ldp_job* job, void* base);

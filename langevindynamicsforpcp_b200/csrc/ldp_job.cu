@@ -280,7 +280,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // FP64 plain jobs hold their whole trajectory state and cell-table rings;
 // FP32 batched jobs hold outputs and the per-trajectory statistics state
 // touched on events (their hot state lives in the persistent slots).
-static size_t job_arena(ldp_job* job, bool alloc) {
+static size_t job_arena(ldp_job* job, bool alloc, void* at = nullptr) {
     const ldp_params* p = &job->p;
     const bool fixed = job->o.mode == LDP_MODE_FIXED_STEPS;
     const bool f32 = job->o.precision == LDP_PREC_FP32_BATCHED;
@@ -316,9 +316,14 @@ static size_t job_arena(ldp_job* job, bool alloc) {
     // Stream-ordered allocation from the device pool: jobs created and freed
     // in a loop reuse the same memory without a device synchronization.
     cudaStream_t st = job->ctx->stream;
-    if (cudaMallocAsync(&job->arena, off, st) != cudaSuccess) {
+    if (at) {
+        job->arena = at;
+        job->arena_owned = false;
+    } else if (cudaMallocAsync(&job->arena, off, st) != cudaSuccess) {
         job->arena = nullptr;
         return 0;
+    } else {
+        job->arena_owned = true;
     }
     cudaMemsetAsync(job->arena, 0, off, st);
     char* a = (char*)job->arena;
@@ -362,6 +367,7 @@ static size_t job_arena(ldp_job* job, bool alloc) {
 }
 
 size_t ldp_job_arena(ldp_job* job, bool alloc) { return job_arena(job, alloc); }
+size_t ldp_job_arena_at(ldp_job* job, void* base) { return job_arena(job, true, base); }
 
 static ldp_status job_create(ldp_ctx* ctx, const ldp_params* p, const ldp_job_opts* o, ldp_job** out, bool check_mem);
 
@@ -651,7 +657,7 @@ extern "C" void ldp_job_destroy(ldp_job* job) {
     if (job->gexec) cudaGraphExecDestroy(job->gexec);
     for (int i = 0; i < 4; ++i)
         if (job->ev[i]) cudaEventDestroy(job->ev[i]);
-    if (job->arena) cudaFreeAsync(job->arena, job->ctx->stream);
+    if (job->arena && job->arena_owned) cudaFreeAsync(job->arena, job->ctx->stream);
     delete job;
 }
 

@@ -5,7 +5,9 @@
 //  1. admits queued jobs while their device footprint fits the memory
 //     budget, oldest first, letting later jobs that fit pass one that does
 //     not for at most kBypassWindow (a job larger than the whole budget is
-//     admitted alone), allocating their arena and registering them with the
+//     admitted alone), placing their arena in the server's device region
+//     (allocated once: no device allocation per job, which can stall the
+//     loop for seconds while the pool grows) and registering them with the
 //     work queue of their model type;
 //  2. publishes admitted jobs' trajectories to the queue in chunks, keeping
 //     about half a wave of slots' worth of unclaimed work queued and always
@@ -35,6 +37,7 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -51,10 +54,53 @@ double now_s() {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+// First-fit placement of job arenas in one device region, with coalescing
+// of free neighbours.  Offsets and sizes are multiples of 256 bytes.
+class Region {
+   public:
+    void reset(size_t cap) {
+        free_.clear();
+        if (cap) free_[0] = cap;
+    }
+    // Offset of a free block of `bytes`, or kNone.
+    size_t take(size_t bytes) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            const size_t off = it->first, left = it->second - bytes;
+            free_.erase(it);
+            if (left) free_[off + bytes] = left;
+            return off;
+        }
+        return kNone;
+    }
+    void give(size_t off, size_t bytes) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        auto nx = free_.lower_bound(off);
+        if (nx != free_.end() && off + bytes == nx->first) {
+            bytes += nx->second;
+            nx = free_.erase(nx);
+        }
+        if (nx != free_.begin()) {
+            auto pv = std::prev(nx);
+            if (pv->first + pv->second == off) {
+                pv->second += bytes;
+                return;
+            }
+        }
+        free_[off] = bytes;
+    }
+    static constexpr size_t kNone = ~(size_t)0;
+
+   private:
+    std::map<size_t, size_t> free_;   // offset -> size
+};
+
 struct Entry {
     uint64_t ticket = 0;
     ldp_job* job = nullptr;
     size_t bytes = 0;
+    size_t offset = Region::kNone;   // arena's place in the server's region
     int state = LDP_SRV_QUEUED;
     int type = -1;
     uint64_t gen_admit = 0;          // remaining-counter copies issued before admission
@@ -67,6 +113,8 @@ struct Entry {
 struct ldp_server {
     ldp_ctx* ctx = nullptr;
     size_t budget = 0, in_use = 0;
+    char* region = nullptr;              // device memory of the job arenas (budget bytes)
+    Region placer;
     uint32_t pair_budget = 0;
     int max_inflight = 2;
     cudaStream_t side = nullptr;         // post-processing
@@ -85,6 +133,23 @@ struct ldp_server {
     std::deque<cudaEvent_t> inflight[4];
     std::vector<cudaEvent_t> pool;       // idle events
     int64_t launches = 0;
+    int64_t steps = 0;
+    double phase_s[6] = {}, phase_max_s[6] = {};   // host time per phase of a step
+    double phase_cur[6] = {};                       // of the current step
+
+    // Adds the time since t0 to phase i of the current step; t0 = now.
+    void phase(int i, double& t0) {
+        const double t = now_s();
+        phase_cur[i] += t - t0;
+        t0 = t;
+    }
+    void close_step() {
+        for (int i = 0; i < 6; ++i) {
+            phase_s[i] += phase_cur[i];
+            phase_max_s[i] = std::max(phase_max_s[i], phase_cur[i]);
+            phase_cur[i] = 0;
+        }
+    }
 
     cudaEvent_t get_event() {
         if (!pool.empty()) {
@@ -109,6 +174,7 @@ extern "C" void ldp_server_opts_default(ldp_server_opts* o) {
     o->hbm_budget = 0;        // 80% of the free device memory at creation
     o->pair_budget = 1024;    // step pairs per slot per launch
     o->max_inflight = 2;
+    o->region = 1;
 }
 
 extern "C" ldp_status ldp_server_create(ldp_ctx* ctx, const ldp_server_opts* o, ldp_server** out) {
@@ -124,7 +190,16 @@ extern "C" ldp_status ldp_server_create(ldp_ctx* ctx, const ldp_server_opts* o, 
     s->ctx = ctx;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    s->budget = opts.hbm_budget ? (size_t)opts.hbm_budget : (size_t)(0.8 * (double)free_b);
+    // Job arenas come from the device's stream-ordered pool (ldp_create keeps
+    // freed memory in it): memory the pool holds unused counts as free.
+    cudaMemPool_t pool = nullptr;
+    uint64_t held = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    }
+    const size_t avail = free_b + (size_t)(held > used ? held - used : 0);
+    s->budget = opts.hbm_budget ? (size_t)opts.hbm_budget : (size_t)(0.8 * (double)avail);
     s->pair_budget = opts.pair_budget ? (uint32_t)opts.pair_budget : 1024u;
     s->max_inflight = opts.max_inflight;
     // Post-processing runs at the highest stream priority: the persistent
@@ -143,6 +218,21 @@ extern "C" ldp_status ldp_server_create(ldp_ctx* ctx, const ldp_server_opts* o, 
         ldp_server_destroy(s);
         ldp_set_error(ctx, "server set-up failed: %s", cudaGetErrorString(e));
         return LDP_ERR_DEVICE;
+    }
+    if (opts.region) {
+        // Memory the pool holds unused goes back to the device first.
+        if (pool && held > used) {
+            cudaDeviceSynchronize();
+            cudaMemPoolTrimTo(pool, 0);
+        }
+        s->budget &= ~(size_t)255;
+        if (cudaMalloc((void**)&s->region, s->budget) != cudaSuccess) {
+            cudaGetLastError();
+            ldp_server_destroy(s);
+            ldp_set_error(ctx, "server region of %zu bytes: device allocation failed", s->budget);
+            return LDP_ERR_NOMEM;
+        }
+        s->placer.reset(s->budget);
     }
     *out = s;
     return LDP_OK;
@@ -179,11 +269,13 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
     int done = 0;
+    ++s->steps;
 
     // 1. admission by footprint, oldest first; a later job that fits may
     //    pass one that does not, unless the oldest pending job has waited
     //    longer than the bypass window (then it is admitted next).
     const double t_now = now_s();
+    double tp = t_now;
     for (size_t i = 0;;) {
         Entry* en = nullptr;
         size_t pos = 0;
@@ -203,7 +295,28 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
             }
         }
         ldp_job* job = en->job;
-        if (ldp_job_arena(job, true) == 0) {
+        bool got = false;
+        if (s->region && en->bytes <= s->budget) {
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                en->offset = s->placer.take(en->bytes);
+            }
+            got = en->offset != Region::kNone;
+            if (got) ldp_job_arena_at(job, s->region + en->offset);
+        } else {
+            // no region, or a job larger than the whole budget (admitted
+            // alone): its own allocation
+            got = ldp_job_arena(job, true) != 0;
+        }
+        s->phase(0, tp);
+        if (!got && s->region && en->bytes <= s->budget) {
+            // the region is fragmented or held by finished jobs not yet
+            // released: wait for releases
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->pending.insert(s->pending.begin() + (std::ptrdiff_t)pos, en);
+            break;
+        }
+        if (!got) {
             const bool idle = s->running.empty() && s->finishing.empty();
             if (idle) {
                 en->state = LDP_SRV_FAILED;
@@ -223,15 +336,21 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         cudaStreamWaitEvent(s->qs[en->type], ready, 0);
         s->pool.push_back(ready);
         const int e = ldp::fp32_register(job, s->qs[en->type], false);
+        s->phase(1, tp);
         if (e) return fail(s, "job registration", (cudaError_t)e);
         job->submitted = true;
         job->fp32_phase = 1;
         en->state = LDP_SRV_RUNNING;
         en->gen_admit = s->rem_gen[en->type];
         en->t_admit = now_s();
-        s->in_use += en->bytes;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->in_use += en->bytes;
+        }
         s->running.push_back(en);
     }
+
+    s->phase(0, tp);
 
     // 2. publication: about one wave of unclaimed work per type, shortest
     //    remaining job first
@@ -258,6 +377,8 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         }
     }
 
+    s->phase(2, tp);
+
     // 3. persistent launches of every type with work
     for (int t = 0; t < 4; ++t) {
         auto& q = s->inflight[t];
@@ -275,6 +396,8 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
             q.push_back(ev);
         }
     }
+
+    s->phase(3, tp);
 
     // 4. completion: one counter copy per type, read when it has landed
     for (int t = 0; t < 4; ++t) {
@@ -318,6 +441,8 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         }
     }
 
+    s->phase(4, tp);
+
     // 5. jobs whose post-processing ran
     for (size_t i = 0; i < s->finishing.size();) {
         Entry* en = s->finishing[i];
@@ -336,6 +461,8 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         s->finishing[i] = s->finishing.back();
         s->finishing.pop_back();
     }
+    s->phase(5, tp);
+    s->close_step();
     if (ndone) *ndone = done;
     return LDP_OK;
 }
@@ -385,8 +512,12 @@ extern "C" ldp_status ldp_server_release(ldp_server* s, uint64_t ticket) {
         if (en->state != LDP_SRV_DONE && en->state != LDP_SRV_FAILED) return LDP_ERR_NOT_READY;
         s->all.erase(it);
     }
-    if (en->state == LDP_SRV_DONE) s->in_use -= en->bytes;
     ldp_job_destroy(en->job);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (en->state == LDP_SRV_DONE) s->in_use -= en->bytes;
+        if (en->offset != Region::kNone) s->placer.give(en->offset, en->bytes);
+    }
     delete en;
     return LDP_OK;
 }
@@ -404,6 +535,11 @@ extern "C" ldp_status ldp_server_info_get(ldp_server* s, ldp_server_info* info) 
     info->hbm_in_use = (int64_t)s->in_use;
     info->hbm_budget = (int64_t)s->budget;
     info->launches = s->launches;
+    info->steps = s->steps;
+    for (int i = 0; i < 6; ++i) {
+        info->phase_s[i] = s->phase_s[i];
+        info->phase_max_s[i] = s->phase_max_s[i];
+    }
     return LDP_OK;
 }
 
@@ -437,6 +573,7 @@ extern "C" void ldp_server_destroy(ldp_server* s) {
         if (s->h_rem[t]) cudaFreeHost(s->h_rem[t]);
     }
     for (cudaEvent_t e : s->pool) cudaEventDestroy(e);
+    if (s->region) cudaFree(s->region);
     if (s->side) cudaStreamDestroy(s->side);
     for (int t = 0; t < 4; ++t)
         if (s->qs[t]) cudaStreamDestroy(s->qs[t]);

@@ -28,7 +28,7 @@ def test_library_exports_every_declared_function():
     for n in names:
         assert hasattr(h, n), n
         assert n in L.SIGNATURES, f"{n} has no ctypes signature"
-    assert h.ldp_abi_version() == 1
+    assert h.ldp_abi_version() == L.ABI_VERSION == 2
 
 
 def test_status_strings():
