@@ -6,7 +6,8 @@ results must be the same alone and in the mix: the test runs a staggered
 stream of mixed jobs through the server and compares each job, bit for bit,
 with the same job run alone through ldp_submit.  A second test gives the
 server a memory budget that holds about two jobs and checks that the bytes
-admitted never exceed it while every job still completes.
+admitted never exceed it while every job still completes, and that the
+space of released jobs is whole again afterwards.
 """
 import numpy as np
 import pytest
@@ -67,3 +68,17 @@ def test_admission_respects_the_memory_budget():
                     break
             assert len(done) == len(tickets)
             assert peak >= min(sizes)
+            # Arenas live in the server's region: released jobs give their
+            # space back and freed neighbours merge, so a job of about twice
+            # the largest one above (the region holds 2.2x) is placed.
+            assert srv.info()["hbm_in_use"] == 0
+            big = max(range(len(work)), key=lambda i: sizes[i])
+            p, n, _ = work[big]
+            t = srv.submit(p, 2 * n, job_id=100)
+            for _ in range(200000):
+                srv.step()
+                if srv.poll(t)[0] == L.SRV_DONE:
+                    break
+            assert srv.poll(t)[0] == L.SRV_DONE
+            assert sizes[big] < srv.info()["hbm_in_use"] <= budget
+            srv.release(t)
