@@ -37,13 +37,13 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
-#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
 
 #include "ldp_fp32.h"
 #include "ldp_internal.h"
+#include "ldp_region.h"
 
 namespace {
 
@@ -54,53 +54,11 @@ double now_s() {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-// First-fit placement of job arenas in one device region, with coalescing
-// of free neighbours.  Offsets and sizes are multiples of 256 bytes.
-class Region {
-   public:
-    void reset(size_t cap) {
-        free_.clear();
-        if (cap) free_[0] = cap;
-    }
-    // Offset of a free block of `bytes`, or kNone.
-    size_t take(size_t bytes) {
-        bytes = (bytes + 255) & ~(size_t)255;
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < bytes) continue;
-            const size_t off = it->first, left = it->second - bytes;
-            free_.erase(it);
-            if (left) free_[off + bytes] = left;
-            return off;
-        }
-        return kNone;
-    }
-    void give(size_t off, size_t bytes) {
-        bytes = (bytes + 255) & ~(size_t)255;
-        auto nx = free_.lower_bound(off);
-        if (nx != free_.end() && off + bytes == nx->first) {
-            bytes += nx->second;
-            nx = free_.erase(nx);
-        }
-        if (nx != free_.begin()) {
-            auto pv = std::prev(nx);
-            if (pv->first + pv->second == off) {
-                pv->second += bytes;
-                return;
-            }
-        }
-        free_[off] = bytes;
-    }
-    static constexpr size_t kNone = ~(size_t)0;
-
-   private:
-    std::map<size_t, size_t> free_;   // offset -> size
-};
-
 struct Entry {
     uint64_t ticket = 0;
     ldp_job* job = nullptr;
     size_t bytes = 0;
-    size_t offset = Region::kNone;   // arena's place in the server's region
+    size_t offset = ldp::Region::kNone;   // arena's place in the server's region
     int state = LDP_SRV_QUEUED;
     int type = -1;
     uint64_t gen_admit = 0;          // remaining-counter copies issued before admission
@@ -114,7 +72,7 @@ struct ldp_server {
     ldp_ctx* ctx = nullptr;
     size_t budget = 0, in_use = 0;
     char* region = nullptr;              // device memory of the job arenas (budget bytes)
-    Region placer;
+    ldp::Region placer;
     uint32_t pair_budget = 0;
     int max_inflight = 2;
     cudaStream_t side = nullptr;         // post-processing
@@ -301,7 +259,7 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
                 std::lock_guard<std::mutex> lk(s->mu);
                 en->offset = s->placer.take(en->bytes);
             }
-            got = en->offset != Region::kNone;
+            got = en->offset != ldp::Region::kNone;
             if (got) ldp_job_arena_at(job, s->region + en->offset);
         } else {
             // no region, or a job larger than the whole budget (admitted
@@ -516,7 +474,7 @@ extern "C" ldp_status ldp_server_release(ldp_server* s, uint64_t ticket) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (en->state == LDP_SRV_DONE) s->in_use -= en->bytes;
-        if (en->offset != Region::kNone) s->placer.give(en->offset, en->bytes);
+        if (en->offset != ldp::Region::kNone) s->placer.give(en->offset, en->bytes);
     }
     delete en;
     return LDP_OK;
