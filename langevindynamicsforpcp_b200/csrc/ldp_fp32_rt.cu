@@ -77,7 +77,8 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
                 al256(sizeof(unsigned long long) * kFp32MaxJobs);
     cudaError_t e = cudaMalloc(&Q.qmem, qb);
     if (e != cudaSuccess) return (int)e;
-    cudaMemset(Q.qmem, 0, qb);
+    e = cudaMemset(Q.qmem, 0, qb);
+    if (e != cudaSuccess) return (int)e;
     char* a = (char*)Q.qmem;
     size_t o = 0;
     Q.q.range_end = (int64_t*)(a + o); o += al256(sizeof(int64_t) * kFp32MaxRanges);
@@ -96,7 +97,8 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
                 al256(sizeof(unsigned long long));
     e = cudaMalloc(&Q.smem, sb);
     if (e != cudaSuccess) return (int)e;
-    cudaMemset(Q.smem, 0, sb);
+    e = cudaMemset(Q.smem, 0, sb);
+    if (e != cudaSuccess) return (int)e;
     a = (char*)Q.smem;
     o = 0;
     SlotsDev& S = Q.s;
@@ -121,7 +123,8 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     S.retired = (unsigned long long*)(a + o);
     // every slot starts empty
     std::vector<int32_t> neg((size_t)nslots, -1);
-    cudaMemcpy(S.job, neg.data(), sizeof(int32_t) * nslots, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(S.job, neg.data(), sizeof(int32_t) * nslots, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return (int)e;
     e = cudaMallocHost((void**)&Q.h_stage, 4096 * Fp32Queue::kStageSlots);
     if (e != cudaSuccess) return (int)e;
     for (int i = 0; i < Fp32Queue::kStageSlots; ++i) {

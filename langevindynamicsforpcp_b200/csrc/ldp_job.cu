@@ -325,7 +325,11 @@ static size_t job_arena(ldp_job* job, bool alloc, void* at = nullptr) {
     } else {
         job->arena_owned = true;
     }
-    cudaMemsetAsync(job->arena, 0, off, st);
+    if (cudaMemsetAsync(job->arena, 0, off, st) != cudaSuccess) {
+        if (job->arena_owned) cudaFreeAsync(job->arena, st);
+        job->arena = nullptr;
+        return 0;
+    }
     char* a = (char*)job->arena;
     TrajState& S = job->st;
     S.n = n;
@@ -361,8 +365,13 @@ static size_t job_arena(ldp_job* job, bool alloc, void* at = nullptr) {
     job->d_means = (double*)(a + o_mean);
     job->d_ssum = f32 ? (int64_t*)(a + o_ssum) : nullptr;
     job->d_i32b = f32 ? (int32_t*)(a + o_i32b) : nullptr;
-    if (nlag > 0)
-        cudaMemcpyAsync(job->d_lags, job->lags.data(), sizeof(int64_t) * nlag, cudaMemcpyHostToDevice, st);
+    if (nlag > 0 &&
+        cudaMemcpyAsync(job->d_lags, job->lags.data(), sizeof(int64_t) * nlag, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess) {
+        if (job->arena_owned) cudaFreeAsync(job->arena, st);
+        job->arena = nullptr;
+        return 0;
+    }
     return off;
 }
 

@@ -116,7 +116,7 @@ struct ldp_server {
             return e;
         }
         cudaEvent_t e = nullptr;
-        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) e = nullptr;
         return e;
     }
 };
@@ -290,9 +290,11 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         job->launches = 0;
         // the arena was allocated on the context's stream
         cudaEvent_t ready = s->get_event();
-        cudaEventRecord(ready, st);
-        cudaStreamWaitEvent(s->qs[en->type], ready, 0);
+        if (!ready) return fail(s, "event creation", cudaErrorMemoryAllocation);
         s->pool.push_back(ready);
+        cudaError_t ce = cudaEventRecord(ready, st);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s->qs[en->type], ready, 0);
+        if (ce != cudaSuccess) return fail(s, "admission ordering", ce);
         const int e = ldp::fp32_register(job, s->qs[en->type], false);
         s->phase(1, tp);
         if (e) return fail(s, "job registration", (cudaError_t)e);
@@ -350,8 +352,10 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
             if (e) return fail(s, "persistent launch", (cudaError_t)e);
             ++s->launches;
             cudaEvent_t ev = s->get_event();
-            cudaEventRecord(ev, s->qs[t]);
+            if (!ev) return fail(s, "event creation", cudaErrorMemoryAllocation);
             q.push_back(ev);
+            const cudaError_t ce = cudaEventRecord(ev, s->qs[t]);
+            if (ce != cudaSuccess) return fail(s, "launch event", ce);
         }
     }
 
@@ -378,7 +382,9 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
                 const int e = ldp::fp32_finalize(en->job, s->side);
                 if (e) return fail(s, "post-processing", (cudaError_t)e);
                 en->fin = s->get_event();
-                cudaEventRecord(en->fin, s->side);
+                if (!en->fin) return fail(s, "event creation", cudaErrorMemoryAllocation);
+                const cudaError_t ce = cudaEventRecord(en->fin, s->side);
+                if (ce != cudaSuccess) return fail(s, "post-processing event", ce);
                 en->state = LDP_SRV_FINISHING;
                 en->t_ready = now_s();
                 en->job->fp32_phase = 2;
