@@ -260,11 +260,12 @@ def main():
                 j.wait()
             ctx.mark(1)
             times.append(ctx.elapsed_ms(0, 1))
-            t = jobs[0].timing()
-            kernel_ms.append(t["integrate_ms"])
-            # the jobs' post-processing (event sums, MSD) runs after the batch,
-            # one job after the other: the last one ends post_ms after it
-            msd_ms.append(max(j.timing()["msd_ms"] for j in jobs))
+            # integration ends with the last job's launch bound; each job's
+            # post-processing (event sums, MSD) starts at its own bound, beside
+            # the later jobs' launches, so post_ms is what remains after the
+            # integration
+            kernel_ms.append(max(j.timing()["integrate_ms"] for j in jobs))
+            msd_ms.append(times[-1] - kernel_ms[-1])
             launches += sum(j.timing()["launches"] for j in jobs)
             acc32 = job_summary(jobs[0])
             for j in jobs:

@@ -17,10 +17,9 @@
 
 #include "ldp_fp32.h"
 #include "ldp_internal.h"
+#include "ldp_msd.h"
 
 namespace ldp {
-int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
-               double* msd0, double* msd_sum, void* stream, bool f32);
 
 struct Fp32Queue {
     bool ready = false;
@@ -225,6 +224,15 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
 
 int fp32_type_of(const ldp_job* job) { return (job->k.dbl ? 2 : 0) + (job->k.over ? 1 : 0); }
 
+bool fp32_queue_quiet(ldp_ctx* ctx, int type) {
+    if (!ctx->fp32) return true;
+    const Fp32Queue& Q = ctx->fp32->q[type];
+    if (!Q.ready) return true;
+    for (const ldp_job* j : Q.table)
+        if (j && !j->done) return false;
+    return true;
+}
+
 // One persistent launch of a queue with a given pair budget (serving).
 int fp32_launch_type(ldp_ctx* ctx, int type, uint32_t pair_budget, cudaStream_t st) {
     Fp32Queue& Q = ctx->fp32->q[type];
@@ -355,6 +363,12 @@ int fp32_launch_bound(ldp_ctx* ctx, int type, double total_pairs, double max_pai
     return (int)std::min(n, 1.0e6);
 }
 
+int fp32_snapshot_remaining(ldp_job* job, unsigned long long* dst, cudaStream_t stream) {
+    const Fp32Queue& Q = job->ctx->fp32->q[job->fp32_type];
+    return (int)cudaMemcpyAsync(dst, &Q.rem[job->fp32_slot], sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                stream);
+}
+
 int fp32_remaining(ldp_job* job, unsigned long long* rem) {
     const Fp32Queue& Q = job->ctx->fp32->q[job->fp32_type];
     return (int)cudaMemcpy(rem, &Q.rem[job->fp32_slot], sizeof(unsigned long long), cudaMemcpyDeviceToHost);
@@ -366,8 +380,9 @@ __global__ void ssum_to_time_kernel(const int64_t* ssum, double* sums, double dt
 }
 
 // Post-processing after all trajectories retired: event-duration sums in
-// time units, then the MSD of the saved frames.
-int fp32_finalize(ldp_job* job, cudaStream_t stream) {
+// time units, then the MSD of the saved frames (lean: the MSD instance that
+// fits beside running persistent blocks; same results).
+int fp32_finalize(ldp_job* job, cudaStream_t stream, bool lean) {
     cudaStream_t st = stream ? stream : job->ctx->stream;
     const int64_t n = (int64_t)LDP_NSUM * job->ntraj;
     ssum_to_time_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(job->d_ssum, job->st.sums, job->k.dt, n);
@@ -376,7 +391,7 @@ int fp32_finalize(ldp_job* job, cudaStream_t stream) {
     ++job->launches;
     if (job->o.mode == LDP_MODE_FIXED_STEPS && !job->lags.empty()) {
         e = launch_msd(job->st.fx, job->nframe, job->ntraj, job->d_lags, (int64_t)job->lags.size(), job->d_msd0,
-                       job->d_msd, st, true);
+                       job->d_msd, st, lean ? LDP_MSD_FP32_LEAN : LDP_MSD_FP32);
         if (e) return e;
         job->launches += 2;
     }

@@ -28,6 +28,7 @@ struct ldp_ctx {
     int fp32_blocks_per_sm = 0;    // resident blocks per SM (0: default 4)
     uint64_t fp32_pair_budget = 0; // step pairs per slot per launch (0: default)
     int fp32_ring_slots = 0;       // cell-table ring slots per slot (0: default 64)
+    cudaStream_t side = nullptr;   // post-processing beside running batches (high priority)
 };
 
 struct ldp_job {
@@ -59,6 +60,7 @@ struct ldp_job {
     cudaGraphExec_t gexec = nullptr;   // batch graph this job owns (first job of the batch)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool submitted = false;
+    bool rem_snapshot = false;   // FP32 batched: counter copied to d_aux before post-processing
     bool done = false;
     int64_t launches = 0;
     int64_t steps_total = 0;
@@ -85,7 +87,12 @@ int fp32_copy_remaining(ldp_ctx* ctx, int type, unsigned long long* host, unsign
                         cudaStream_t st);
 int64_t fp32_nslots(ldp_ctx* ctx, int type);
 unsigned long long fp32_published(ldp_ctx* ctx, int type);
-int fp32_finalize(ldp_job* job, cudaStream_t stream = nullptr);
+int fp32_finalize(ldp_job* job, cudaStream_t stream = nullptr, bool lean = false);
+// Whether every job in the type's queue has finished (or it has none): the
+// queue's items are then exactly those published after this call.
+bool fp32_queue_quiet(ldp_ctx* ctx, int type);
+// Stream-ordered copy of the job's "not yet retired" counter to dst.
+int fp32_snapshot_remaining(ldp_job* job, unsigned long long* dst, cudaStream_t stream);
 void fp32_release(ldp_job* job);
 void fp32_destroy_runtime(ldp_ctx* ctx);
 }  // namespace ldp

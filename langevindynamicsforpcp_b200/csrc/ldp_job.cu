@@ -19,12 +19,7 @@
 
 #include "ldp_engine.h"
 #include "ldp_internal.h"
-
-namespace ldp {
-int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
-               double* msd0, double* msd_sum, void* stream, bool f32);
-int launch_traj_means(const int64_t* counts, const double* sums, double* means, int64_t n, int ncg, void* stream);
-}  // namespace ldp
+#include "ldp_msd.h"
 
 using namespace ldp;
 
@@ -102,6 +97,10 @@ extern "C" void ldp_destroy(ldp_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
     fp32_destroy_runtime(ctx);
     for (int i = 0; i < kCtxMarks; ++i)
         if (ctx->marks[i]) cudaEventDestroy(ctx->marks[i]);
@@ -537,7 +536,7 @@ extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
     }
     if (job->o.mode == LDP_MODE_FIXED_STEPS && !job->lags.empty()) {
         int e = launch_msd(job->st.fx, job->nframe, job->ntraj, job->d_lags, (int64_t)job->lags.size(), job->d_msd0,
-                           job->d_msd, s, false);
+                           job->d_msd, s, LDP_MSD_FP64);
         if (e) {
             ldp_set_error(ctx, "MSD launch failed: %s", cudaGetErrorString((cudaError_t)e));
             return LDP_ERR_DEVICE;
@@ -570,12 +569,17 @@ static ldp_status fp32_advance(ldp_ctx* ctx, ldp_job* job, int* done) {
         return LDP_OK;
     }
     if (job->fp32_phase == 3) {
-        // The batch graph ran every launch its bound allows and the
-        // post-processing after them; all trajectories must have retired.
+        // The batch ran every launch its bound allows before the job's
+        // post-processing; all trajectories must have retired by then (the
+        // counter as copied just before the post-processing, when taken).
         unsigned long long rem = 0;
-        CUDA_OR_FAIL(ctx, (cudaError_t)fp32_remaining(job, &rem));
+        if (job->rem_snapshot) {
+            CUDA_OR_FAIL(ctx, cudaMemcpy(&rem, job->d_aux, sizeof(rem), cudaMemcpyDeviceToHost));
+        } else {
+            CUDA_OR_FAIL(ctx, (cudaError_t)fp32_remaining(job, &rem));
+        }
         if (rem > 0) {
-            ldp_set_error(ctx, "batch graph ended with %llu trajectories not retired", rem);
+            ldp_set_error(ctx, "%llu trajectories not retired after the batch's launch bound", rem);
             return LDP_ERR_DEVICE;
         }
     }
@@ -800,6 +804,21 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
         }
     int launches[4] = {0, 0, 0, 0};
     ldp_job* first[4] = {nullptr, nullptr, nullptr, nullptr};
+    // A type whose queue holds no unfinished job gets each job's
+    // post-processing as soon as that job has surely retired: items are
+    // claimed in publication order by slots that never idle while items
+    // remain, so a list-scheduling bound on the launches that drain the
+    // jobs published so far (fp32_launch_bound of the prefix) holds per
+    // job.  The post-processing then runs on a side stream beside the
+    // later jobs' launches, in the registers and shared memory three
+    // persistent blocks leave on an SM.
+    bool early[4];
+    for (int t = 0; t < 4; ++t) early[t] = fp32_queue_quiet(ctx, t);
+    for (int i = 0; i < njobs; ++i)   // first-passage jobs: no tight bound
+        if (jobs[i]->o.precision == LDP_PREC_FP32_BATCHED && jobs[i]->o.mode != LDP_MODE_FIXED_STEPS)
+            early[fp32_type_of(jobs[i])] = false;
+    std::vector<int> bound(njobs, 0);
+    double prefix[4] = {0, 0, 0, 0}, longest[4] = {0, 0, 0, 0};
     for (int i = 0; i < njobs; ++i) {
         ldp_job* job = jobs[i];
         if (job->o.precision != LDP_PREC_FP32_BATCHED) continue;
@@ -818,18 +837,45 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
         const int t = job->fp32_type;
         launches[t] += fp32_estimate_launches(job);
         if (!first[t]) first[t] = job;
+        if (early[t]) {
+            const double pairs = (double)((job->nsteps + 1) / 2);
+            prefix[t] += pairs * (double)job->ntraj;
+            longest[t] = std::max(longest[t], pairs);
+            bound[i] = fp32_launch_bound(ctx, t, prefix[t], longest[t]);
+            launches[t] = std::max(launches[t], bound[i]);
+        }
     }
-    for (int t = 0; t < 4; ++t)
-        if (first[t]) {
-            int e = fp32_pump(first[t], launches[t]);
+    if (!ctx->side && (early[0] || early[1] || early[2] || early[3])) {
+        int lo_prio = 0, hi_prio = 0;
+        cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+        CUDA_OR_FAIL(ctx, cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, hi_prio));
+    }
+    for (int t = 0; t < 4; ++t) {
+        if (!first[t]) continue;
+        for (int k = 1; k <= launches[t]; ++k) {
+            int e = fp32_pump(first[t], 1);
             if (e) {
                 ldp_set_error(ctx, "FP32 launch failed: %s", cudaGetErrorString((cudaError_t)e));
                 return LDP_ERR_DEVICE;
             }
+            if (!early[t]) continue;
+            for (int i = 0; i < njobs; ++i) {
+                ldp_job* job = jobs[i];
+                if (job->o.precision != LDP_PREC_FP32_BATCHED || job->fp32_type != t || bound[i] != k) continue;
+                CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[1], s));
+                CUDA_OR_FAIL(ctx, cudaStreamWaitEvent(ctx->side, job->ev[1], 0));
+                CUDA_OR_FAIL(ctx, (cudaError_t)fp32_snapshot_remaining(job, (unsigned long long*)job->d_aux,
+                                                                       ctx->side));
+                job->rem_snapshot = true;
+                CUDA_OR_FAIL(ctx, (cudaError_t)fp32_finalize(job, ctx->side, true));
+                CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[2], ctx->side));
+                job->fp32_phase = 3;   // checked when waited on: every trajectory retired
+            }
         }
+    }
     for (int i = 0; i < njobs; ++i) {
         ldp_job* job = jobs[i];
-        if (job->o.precision != LDP_PREC_FP32_BATCHED) continue;
+        if (job->o.precision != LDP_PREC_FP32_BATCHED || early[job->fp32_type]) continue;
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[1], s));
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[2], s));
         job->fp32_phase = 1;

@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "../../include/ldp.h"
+#include "ldp_msd.h"
 
 namespace ldp {
 
@@ -41,7 +42,12 @@ constexpr int kMsdSmemBytes = 100 * 1024;   // two blocks per SM
 constexpr int kMsdBlock = 256;
 constexpr int kMsdLags = 4;                  // lags per work item (x[k] reuse)
 constexpr int kMsdF32SmemBytes = 54 * 1024;  // FP32 kernel: four blocks per SM
-constexpr int kMsdF32Lags = 8;
+// Lean FP32 instance (msd_smem_f32_kernel<128, 4, 16, true>), for
+// post-processing that runs beside the persistent FP32 kernel: one warp per
+// SMSP at 32 registers is what three persistent blocks leave of an SM's
+// register file, and one staged trajectory (12 KB at 3001 frames) fits in
+// its spare shared memory.  Every lag is summed in the same order, so its
+// results equal the full instance's bit for bit.
 
 __global__ void __launch_bounds__(kMsdBlock) msd_smem_kernel(const double* __restrict__ frames, int nframe,
                                                              int64_t ntraj, int G, const int64_t* __restrict__ lags,
@@ -98,35 +104,37 @@ __global__ void __launch_bounds__(kMsdBlock) msd_smem_kernel(const double* __res
     }
 }
 
-__global__ void __launch_bounds__(kMsdBlock, 4) msd_smem_f32_kernel(const double* __restrict__ frames, int nframe,
-                                                                    int64_t ntraj, int G,
+template <int kBlk, int kNL, int kMinB, bool kOne>
+__global__ void __launch_bounds__(kBlk, kMinB) msd_smem_f32_kernel(const double* __restrict__ frames, int nframe,
+                                                                    int64_t ntraj, int G_,
                                                                     const int64_t* __restrict__ lags, int nlag,
                                                                     double* __restrict__ msd0) {
     extern __shared__ float fs32[];   // [G][nframe]
+    const int G = kOne ? 1 : G_;      // kOne: one trajectory per block
     const int64_t t0 = (int64_t)blockIdx.x * G;
     const int gh = (int)((ntraj - t0) < G ? (ntraj - t0) : G);
     const int total = nframe * G;
-    for (int e = threadIdx.x; e < total; e += kMsdBlock) {
+    for (int e = threadIdx.x; e < total; e += kBlk) {
         const int k = e / G;
         const int j = e - k * G;
         fs32[j * nframe + k] = (j < gh) ? (float)(frames[(int64_t)k * ntraj + t0 + j] - frames[t0 + j]) : 0.0f;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ngroup = (nlag + kMsdF32Lags - 1) / kMsdF32Lags;
+    const int ngroup = (nlag + kNL - 1) / kNL;
     const int items = gh * ngroup;
-    for (int it = warp; it < items; it += kMsdBlock / 32) {
+    for (int it = warp; it < items; it += kBlk / 32) {
         const int j = it / ngroup;
-        const int g0 = (it - j * ngroup) * kMsdF32Lags;
+        const int g0 = (it - j * ngroup) * kNL;
         const float* x = fs32 + j * nframe;
-        int lag[kMsdF32Lags], cnt[kMsdF32Lags];
-        float acc[kMsdF32Lags];
+        int lag[kNL], cnt[kNL];
+        float acc[kNL];
         // Slots past the last lag repeat the group's first lag (results not
         // written), so that kmin is the shortest origin count of real lags.
         const int lag0 = (int)lags[g0];
         int kmin = 1 << 30, kmax = 0;
 #pragma unroll
-        for (int r = 0; r < kMsdF32Lags; ++r) {
+        for (int r = 0; r < kNL; ++r) {
             const int i = g0 + r;
             lag[r] = (i < nlag) ? (int)lags[i] : lag0;
             cnt[r] = nframe - lag[r];
@@ -140,7 +148,7 @@ __global__ void __launch_bounds__(kMsdBlock, 4) msd_smem_f32_kernel(const double
         for (; k < kmin; k += 32) {
             const float xk = x[k];
 #pragma unroll
-            for (int r = 0; r < kMsdF32Lags; ++r) {
+            for (int r = 0; r < kNL; ++r) {
                 const float d = x[k + lag[r]] - xk;
                 acc[r] = fmaf(d, d, acc[r]);
             }
@@ -148,7 +156,7 @@ __global__ void __launch_bounds__(kMsdBlock, 4) msd_smem_f32_kernel(const double
         for (; k < kmax; k += 32) {
             const float xk = x[k];
 #pragma unroll
-            for (int r = 0; r < kMsdF32Lags; ++r) {
+            for (int r = 0; r < kNL; ++r) {
                 if (k < cnt[r]) {
                     const float d = x[k + lag[r]] - xk;
                     acc[r] = fmaf(d, d, acc[r]);
@@ -156,7 +164,7 @@ __global__ void __launch_bounds__(kMsdBlock, 4) msd_smem_f32_kernel(const double
             }
         }
 #pragma unroll
-        for (int r = 0; r < kMsdF32Lags; ++r) {
+        for (int r = 0; r < kNL; ++r) {
             float v = acc[r];
 #pragma unroll
             for (int h = 16; h >= 1; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
@@ -246,21 +254,34 @@ int launch_traj_means(const int64_t* counts, const double* sums, double* means, 
 }
 
 int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_t* lags, int64_t nlag,
-               double* msd0, double* msd_sum, void* stream, bool f32) {
+               double* msd0, double* msd_sum, void* stream, int mode) {
     cudaStream_t s = (cudaStream_t)stream;
+    const bool f32 = mode != LDP_MSD_FP64;
+    const bool lean = mode == LDP_MSD_FP32_LEAN;
     const int64_t per_traj = nframe * (int64_t)(f32 ? sizeof(float) : sizeof(double));
-    int G = (int)((f32 ? kMsdF32SmemBytes : kMsdSmemBytes) / (per_traj > 0 ? per_traj : 1));
-    if (f32 && G < 1 && per_traj <= kMsdSmemBytes) G = 1;
-    if (G > 32) G = 32;
+    int G;
+    if (lean) {
+        // one trajectory per block (kOne), or the global-memory kernel
+        G = per_traj <= kMsdSmemBytes ? 1 : 0;
+    } else {
+        G = (int)((f32 ? kMsdF32SmemBytes : kMsdSmemBytes) / (per_traj > 0 ? per_traj : 1));
+        if (f32 && G < 1 && per_traj <= kMsdSmemBytes) G = 1;
+        if (G > 32) G = 32;
+    }
     cudaError_t e;
     if (G >= 1 && nframe < (1 << 30) && nlag < (1 << 30)) {
         const size_t smem = (size_t)G * (size_t)per_traj;
         const int64_t nblk = (ntraj + G - 1) / G;
-        if (f32) {
-            e = cudaFuncSetAttribute(msd_smem_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (lean) {
+            auto* kern = msd_smem_f32_kernel<128, 4, 16, true>;
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return (int)e;
-            msd_smem_f32_kernel<<<(unsigned)nblk, kMsdBlock, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag,
-                                                                       msd0);
+            kern<<<(unsigned)nblk, 128, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag, msd0);
+        } else if (f32) {
+            auto* kern = msd_smem_f32_kernel<kMsdBlock, 8, 4, false>;
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return (int)e;
+            kern<<<(unsigned)nblk, kMsdBlock, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag, msd0);
         } else {
             e = cudaFuncSetAttribute(msd_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return (int)e;
