@@ -818,6 +818,7 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
         if (jobs[i]->o.precision == LDP_PREC_FP32_BATCHED && jobs[i]->o.mode != LDP_MODE_FIXED_STEPS)
             early[fp32_type_of(jobs[i])] = false;
     std::vector<int> bound(njobs, 0);
+    int top[4] = {0, 0, 0, 0};
     double prefix[4] = {0, 0, 0, 0}, longest[4] = {0, 0, 0, 0};
     for (int i = 0; i < njobs; ++i) {
         ldp_job* job = jobs[i];
@@ -842,9 +843,10 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
             prefix[t] += pairs * (double)job->ntraj;
             longest[t] = std::max(longest[t], pairs);
             bound[i] = fp32_launch_bound(ctx, t, prefix[t], longest[t]);
-            launches[t] = std::max(launches[t], bound[i]);
+            top[t] = std::max(top[t], bound[i]);
         }
     }
+    for (int t = 0; t < 4; ++t) launches[t] = std::max(launches[t], top[t]);
     if (!ctx->side && (early[0] || early[1] || early[2] || early[3])) {
         int lo_prio = 0, hi_prio = 0;
         cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
