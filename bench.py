@@ -296,12 +296,16 @@ def main():
     for it in range(args.warmup + args.steps):
         barrier()
         t0 = time.perf_counter()
-        jobs = run_batch(ldp, ctx, params, ldp.PREC_FP32_BATCHED, job_id0)
+        jobs = [ldp.Job(ctx, p, lanes=NTRAJ, precision=ldp.PREC_FP32_BATCHED, job_id=job_id0 + i)
+                for i, p in enumerate(params)]
+        ldp.submit_batch(ctx, jobs)
         b_in = len(jobs) * (C_sizeof_params())
         b_out = 0
         for j in jobs:
-            # the job's results as the reference reports them: per-trajectory
-            # mean event times and the MSD curve
+            # each job's results as the reference reports them (per-trajectory
+            # mean event times and the MSD curve), read as soon as that job is
+            # done, while the later jobs still integrate
+            j.wait()
             means = j.means()
             lags, msd = j.msd()
             b_out += means.nbytes + msd.nbytes

@@ -29,6 +29,7 @@ struct ldp_ctx {
     uint64_t fp32_pair_budget = 0; // step pairs per slot per launch (0: default)
     int fp32_ring_slots = 0;       // cell-table ring slots per slot (0: default 64)
     cudaStream_t side = nullptr;   // post-processing beside running batches (high priority)
+    cudaStream_t rd = nullptr;     // result reads of finished jobs, beside running work
 };
 
 struct ldp_job {

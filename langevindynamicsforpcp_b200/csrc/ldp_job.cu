@@ -97,10 +97,11 @@ extern "C" void ldp_destroy(ldp_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->side) {
-        cudaStreamSynchronize(ctx->side);
-        cudaStreamDestroy(ctx->side);
-    }
+    for (cudaStream_t* x : {&ctx->side, &ctx->rd})
+        if (*x) {
+            cudaStreamSynchronize(*x);
+            cudaStreamDestroy(*x);
+        }
     fp32_destroy_runtime(ctx);
     for (int i = 0; i < kCtxMarks; ++i)
         if (ctx->marks[i]) cudaEventDestroy(ctx->marks[i]);
@@ -761,7 +762,14 @@ extern "C" ldp_status ldp_job_traj_means(ldp_job* job, double* means) {
     }
     ldp_ctx* ctx = job->ctx;
     cudaSetDevice(ctx->device);
-    cudaStream_t s = ctx->stream;
+    // The job is done: its own stream, so that the read does not queue
+    // behind later jobs' launches on the context's stream.
+    if (!ctx->rd) {
+        int lo_prio = 0, hi_prio = 0;
+        cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+        CUDA_OR_FAIL(ctx, cudaStreamCreateWithPriority(&ctx->rd, cudaStreamNonBlocking, hi_prio));
+    }
+    cudaStream_t s = ctx->rd;
     const int e = launch_traj_means(job->st.counts, job->st.sums, job->d_means, job->ntraj, job->p.n_cg, s);
     if (e) {
         ldp_set_error(ctx, "means launch failed: %s", cudaGetErrorString((cudaError_t)e));

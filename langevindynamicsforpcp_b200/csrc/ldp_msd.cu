@@ -247,7 +247,7 @@ int launch_traj_means(const int64_t* counts, const double* sums, double* means, 
     const int nlists = LDP_E_CG0 + ncg;
     const int64_t total = (int64_t)nlists * n;
     if (total == 0) return 0;
-    const int block = 256;
+    const int block = 128;   // one warp per SMSP: fits beside persistent FP32 blocks
     traj_means_kernel<<<(unsigned)((total + block - 1) / block), block, 0, (cudaStream_t)stream>>>(counts, sums, means,
                                                                                                n, nlists);
     return (int)cudaGetLastError();
