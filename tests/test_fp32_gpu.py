@@ -120,6 +120,35 @@ def test_fp32_job_results_same_alone_and_in_a_shared_batch(ctx):
     same(alone, mixed)
 
 
+def test_batch_post_processing_at_each_jobs_launch_bound():
+    # Jobs of different lengths and sizes in one batch, on a context with a
+    # small pair budget (many launches): each job's post-processing starts
+    # after its own launch bound (the list-scheduling bound of the jobs
+    # published up to it), beside the later jobs' launches, and the job's
+    # counter as copied just before it must be zero (checked by wait).
+    # Every result equals the job run alone (which post-processes after its
+    # last launch, with the full MSD instance).
+    ps = [quick(steps=24000, freq=20), quick(steps=120000, freq=40), quick(steps=60000, freq=20, tau=1e-3),
+          quick(steps=48000, freq=40, x0=-0.3)]
+    lanes = [1000, 300, 2000, 700]
+    got = []
+    with ldp.Context(0) as c1:
+        set_shape(c1, 256, 1, 2000)
+        jobs = [ldp.Job(c1, p, lanes=n, precision=ldp.PREC_FP32_BATCHED, job_id=i)
+                for i, (p, n) in enumerate(zip(ps, lanes))]
+        ldp.submit_batch(c1, jobs)
+        for j in jobs:
+            j.wait()
+            r = j.results()
+            r["lags"], r["msd"] = j.msd()
+            got.append(r)
+            j.close()
+    with ldp.Context(0) as c2:
+        for i, (p, n) in enumerate(zip(ps, lanes)):
+            same(got[i], run(c2, p, ldp.PREC_FP32_BATCHED, lanes=n, job_id=i))
+    assert [int(r["counts"][L.C_STEPS].min()) for r in got] == [24000, 120000, 60000, 48000]
+
+
 def test_fp32_first_passage_refill_independent_of_shape():
     p = quick()
     with ldp.Context(0) as c1, ldp.Context(0) as c2:
