@@ -379,7 +379,7 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
                     continue;
                 }
                 cudaStreamWaitEvent(s->side, s->rem_ev[t], 0);
-                const int e = ldp::fp32_finalize(en->job, s->side);
+                const int e = ldp::fp32_finalize(en->job, s->side, true);   // lean MSD: runs beside the launches
                 if (e) return fail(s, "post-processing", (cudaError_t)e);
                 en->fin = s->get_event();
                 if (!en->fin) return fail(s, "event creation", cudaErrorMemoryAllocation);
