@@ -30,6 +30,8 @@ struct ldp_ctx {
     int fp32_ring_slots = 0;       // cell-table ring slots per slot (0: default 64)
     cudaStream_t side = nullptr;   // post-processing beside running batches (high priority)
     cudaStream_t rd = nullptr;     // result reads of finished jobs, beside running work
+    cudaStream_t gside = nullptr;  // side branch captured into batch graphs
+    cudaEvent_t gjoin = nullptr;   // joins that branch back before the capture ends
 };
 
 struct ldp_job {

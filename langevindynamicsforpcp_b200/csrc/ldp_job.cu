@@ -97,11 +97,12 @@ extern "C" void ldp_destroy(ldp_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (cudaStream_t* x : {&ctx->side, &ctx->rd})
+    for (cudaStream_t* x : {&ctx->side, &ctx->rd, &ctx->gside})
         if (*x) {
             cudaStreamSynchronize(*x);
             cudaStreamDestroy(*x);
         }
+    if (ctx->gjoin) cudaEventDestroy(ctx->gjoin);
     fp32_destroy_runtime(ctx);
     for (int i = 0; i < kCtxMarks; ++i)
         if (ctx->marks[i]) cudaEventDestroy(ctx->marks[i]);
@@ -907,6 +908,13 @@ extern "C" ldp_status ldp_submit_batch_graph(ldp_ctx* ctx, ldp_job** jobs, int n
             return LDP_ERR_INVALID;
         }
     }
+    // Per-job post-processing at prefix launch bounds, as in
+    // ldp_submit_batch, captured as a side branch of the graph.
+    bool early[4];
+    for (int t = 0; t < 4; ++t) early[t] = fp32_queue_quiet(ctx, t);
+    for (int i = 0; i < njobs; ++i)
+        if (jobs[i]->o.mode != LDP_MODE_FIXED_STEPS) early[fp32_type_of(jobs[i])] = false;
+    std::vector<int> bound(njobs, 0);
     double total[4] = {0, 0, 0, 0}, longest[4] = {0, 0, 0, 0};
     for (int i = 0; i < njobs; ++i) {
         ldp_job* job = jobs[i];
@@ -925,18 +933,48 @@ extern "C" ldp_status ldp_submit_batch_graph(ldp_ctx* ctx, ldp_job** jobs, int n
         const double pairs = (double)((job->nsteps + 1) / 2);
         total[t] += pairs * (double)job->ntraj;
         longest[t] = std::max(longest[t], pairs);
+        bound[i] = fp32_launch_bound(ctx, t, total[t], longest[t]);
+    }
+    const bool any_early = early[0] || early[1] || early[2] || early[3];
+    if (any_early && !ctx->gside) {
+        int lo_prio = 0, hi_prio = 0;
+        cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+        CUDA_OR_FAIL(ctx, cudaStreamCreateWithPriority(&ctx->gside, cudaStreamNonBlocking, hi_prio));
+        CUDA_OR_FAIL(ctx, cudaEventCreateWithFlags(&ctx->gjoin, cudaEventDisableTiming));
     }
     CUDA_OR_FAIL(ctx, cudaEventRecord(jobs[0]->ev[0], s));
     CUDA_OR_FAIL(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    // Inside the capture errors accumulate: the capture must end either way.
     int e = 0;
+    bool forked = false;
     for (int t = 0; t < 4 && !e; ++t) {
         if (total[t] <= 0.0) continue;
         ldp_job* first = nullptr;
         for (int i = 0; i < njobs; ++i)
             if (jobs[i]->fp32_type == t) { first = jobs[i]; break; }
-        e = fp32_pump(first, fp32_launch_bound(ctx, t, total[t], longest[t]));
+        const int nl = fp32_launch_bound(ctx, t, total[t], longest[t]);
+        for (int k = 1; k <= nl && !e; ++k) {
+            e = fp32_pump(first, 1);
+            if (!early[t]) continue;
+            for (int i = 0; i < njobs && !e; ++i) {
+                ldp_job* job = jobs[i];
+                if (job->fp32_type != t || bound[i] != k) continue;
+                e = (int)cudaEventRecord(job->ev[3], s);
+                if (!e) e = (int)cudaStreamWaitEvent(ctx->gside, job->ev[3], 0);
+                if (!e) e = fp32_snapshot_remaining(job, (unsigned long long*)job->d_aux, ctx->gside);
+                if (!e) e = fp32_finalize(job, ctx->gside, true);
+                job->rem_snapshot = true;
+                forked = true;
+            }
+        }
     }
-    for (int i = 0; i < njobs && !e; ++i) e = fp32_finalize(jobs[i]);
+    for (int i = 0; i < njobs && !e; ++i)
+        if (!early[jobs[i]->fp32_type]) e = fp32_finalize(jobs[i]);
+    if (forked) {
+        const cudaError_t ej = cudaEventRecord(ctx->gjoin, ctx->gside);
+        const cudaError_t ew = ej == cudaSuccess ? cudaStreamWaitEvent(s, ctx->gjoin, 0) : ej;
+        if (!e && ew != cudaSuccess) e = (int)ew;
+    }
     cudaGraph_t graph = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(s, &graph);
     if (e || ec != cudaSuccess) {
