@@ -71,11 +71,16 @@ DOUBLE = ("BARRIERHEIGHTS0 {mid!r} {low!r}\nBARRIERHEIGHTS1 {high!r} {low!r}\nBA
 class Server:
     """The library's serving loop (ldp_server_create ... ldp_server_destroy)."""
 
-    def __init__(self, ctx: Context, hbm_budget: int = 0, pair_budget: int = 1024, max_inflight: int = 2):
+    def __init__(self, ctx: Context, hbm_budget: int = 0, pair_budget: int = 1024, max_inflight: int = 2,
+                 region: bool = True):
+        """hbm_budget: bytes of job arenas resident at once (0: 80 % of the
+        free device memory); region: allocate that budget once as one device
+        region that arenas are placed in (else one pool allocation per job)."""
         self.ctx = ctx
         o = L.ServerOpts()
         L.lib().ldp_server_opts_default(C.byref(o))
         o.hbm_budget, o.pair_budget, o.max_inflight = hbm_budget, pair_budget, max_inflight
+        o.region = int(region)
         h = C.c_void_p()
         _check(L.lib().ldp_server_create(ctx.handle, C.byref(o), C.byref(h)), ctx)
         self.handle = h
