@@ -345,7 +345,7 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": "particle-steps/s, FP32 batched (vs FP64 plain), 1xB200",
+            "metric": METRIC,
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -366,6 +366,10 @@ def main():
         print(json.dumps(line), flush=True)
     ctx.close()
     rep.close()
+
+
+# The metric both arms report (the reference arm on a bounded sample).
+METRIC = "particle-steps/s, FP32 batched (vs FP64 plain), 1xB200"
 
 
 def workload_config(world):
@@ -397,7 +401,7 @@ def bench_reference(args, rank, world):
         if it >= args.warmup:
             vals.append(r["value"])
     value = sum(vals) / len(vals)
-    line = {"impl": "reference", "metric": "particle-steps/s, FP32 batched (vs FP64 plain), 1xB200",
+    line = {"impl": "reference", "metric": METRIC,
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(world),
