@@ -28,3 +28,17 @@ def test_c_examples_compile(tmp_path):
                         "-Werror=incompatible-pointer-types", "-Wno-unused-variable",
                         "-I", os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_cpp_examples_compile(tmp_path):
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```cpp\n(.*?)```", text, flags=re.S)
+    assert blocks
+    body = "\n".join(line for b in blocks for line in b.splitlines() if not line.startswith("#include"))
+    src = tmp_path / "examples.cpp"
+    src.write_text('#include "ldp_engine.hpp"\nint examples(ldp_ctx* ctx, ldp_params p) {\n' + body +
+                   "\nreturn 0;\n}\n")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Wno-unused-variable",
+                        "-I", os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
