@@ -377,21 +377,30 @@ ldp_status  ldp_job_write_outputs(ldp_job *job, const char *dir);
  * that freeing implies), a plugin that may only use the buffers it is given.
  * The caller passes the parameters and its own device buffers for the
  * outputs: d_counts [LDP_NCOUNT][ntraj], d_sums [LDP_NSUM][ntraj],
- * d_x_final [ntraj], and optionally d_frames_x [nframe][ntraj] (NULL: no
- * frames); ntraj = ranks * NUMBEROFRUNS * lanes, at most
- * LDP_NOALLOC_MAX_TRAJ.  The working state lives in one fixed device array
- * of the library (about 6 MB, held by every GPU that loads the library until
- * the process exits); every call overwrites it, so calls whose device work
+ * d_x_final [ntraj], and optionally d_frames_x [nframe][ntraj] with
+ * nframe = NUMBEROFSTEPS / FREQSAVE + 1 (NULL: no frames);
+ * ntraj = ranks * NUMBEROFRUNS * lanes, at most LDP_NOALLOC_MAX_TRAJ.
+ * o->table_slots (cell-table ring slots per trajectory, a power of two from
+ * 16 to LDP_NOALLOC_MAX_SLOTS; ldp_job_opts_default gives 256) is honoured;
+ * larger values are rejected with LDP_ERR_UNSUPPORTED.  o->block_size,
+ * tick_cap and keep_frames are ignored (the FP64 kernels run 128-thread
+ * blocks, as in a job); o->steps_per_launch is honoured as in a job.  The
+ * working state lives in one fixed device array of the library (about
+ * 18.5 MB, held by every GPU that loads the library's module until the
+ * process exits); every call overwrites it, so calls whose device work
  * overlaps (other streams, other host threads) race on it -- serialize them.
- * The first call on a device looks up that array's address; make it before
- * any stream capture.  The work is enqueued on `stream` (NULL: the current
- * device's default stream) on the current device; the call returns without
- * waiting.  Results equal ldp_job_create/ldp_submit with
- * LDP_PREC_FP64_PLAIN for the same params and layout; RANDOMSEED < 0 means
- * seed 0 here, WAITINGTIME and WRITEX series are not produced, fixed-step
- * mode only.  Errors come back as a status and a message in err.
+ * The first call on a device (and the first after a cudaDeviceReset) looks
+ * up that array's address in the current context; make it before any stream
+ * capture.  The work is enqueued on `stream` (NULL: the current device's
+ * default stream) on the current device; the call returns without waiting.
+ * Results equal ldp_job_create/ldp_submit with LDP_PREC_FP64_PLAIN for the
+ * same params, layout and table_slots; RANDOMSEED < 0 means seed 0 here;
+ * WAITINGTIME, WRITEX series and event lists (event_cap != 0) are not
+ * produced, and FP32 precision or first-passage mode is rejected.  Errors
+ * come back as a status and a message in err.
  */
 #define LDP_NOALLOC_MAX_TRAJ 4096
+#define LDP_NOALLOC_MAX_SLOTS 256
 ldp_status  ldp_integrate_fp64_noalloc(const ldp_params *p, const ldp_job_opts *o, int64_t *d_counts,
                                        double *d_sums, double *d_x_final, double *d_frames_x,
                                        void *stream, char *err, size_t errlen);

@@ -30,6 +30,7 @@ FLAG_NONFINITE, FLAG_TICK_OVERFLOW, FLAG_CENSORED, FLAG_EVENT_OVERFLOW = 1, 2, 4
 # enum ldp_event_list
 E_FPT, E_FPT2, E_TPT, E_TPT2, E_CG0 = range(5)
 NOALLOC_MAX_TRAJ = 4096
+NOALLOC_MAX_SLOTS = 256
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "device error", 4: "timeout",
           5: "i/o error", 6: "parse error", 7: "unsupported", 8: "not ready", 9: "restart error"}

@@ -8,14 +8,17 @@
 // hands them.  The caller passes the parameters and its own device buffers
 // for the outputs; the per-trajectory working state the integration needs
 // (positions, statistics state, cell-table rings) lives in one file-scope
-// device array of fixed size, kLdpNoallocScratchBytes, that every GPU which
-// loads this library holds until the process exits.
+// device array of fixed size, kScratchBytes, that every GPU which loads this
+// library's module holds until the process exits.
 //
-// The kernels are the FP64 plain kernels of ldp_fp64.cu, run exactly as a
-// job runs them, so the outputs equal those of ldp_job_create/ldp_submit for
-// the same parameters and layout.
+// The kernels are the FP64 plain kernels of ldp_fp64.cu, launched with the
+// same cell-table ring size and the same launch chunking a job uses, so the
+// outputs equal those of ldp_job_create/ldp_submit for the same parameters,
+// layout and table_slots.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -23,17 +26,55 @@
 
 namespace {
 
-constexpr int kSlots = 64;                       // cell-table ring slots per trajectory
-constexpr int64_t kPerTraj = 9 * 8 + 9 * 8 + 4 * 4 + 2 * LDP_MAX_CG * 8 + 2 * kSlots * 8;
-constexpr size_t kLdpNoallocScratchBytes = (size_t)LDP_NOALLOC_MAX_TRAJ * kPerTraj + 64 * 256;
+// Bytes of working state per trajectory at `slots` cell-table ring slots:
+// 9 FP64 and 9 int64 fields, 4 int32 fields, the FPTCG clocks and wells and
+// the ring's tags and data.
+constexpr int64_t per_traj_bytes(int64_t slots) {
+    return 9 * 8 + 9 * 8 + 4 * 4 + 2 * LDP_MAX_CG * 8 + 2 * slots * 8;
+}
+// 12 arrays, each padded to 256 bytes.
+constexpr size_t kScratchBytes =
+    (size_t)LDP_NOALLOC_MAX_TRAJ * per_traj_bytes(LDP_NOALLOC_MAX_SLOTS) + 12 * 256;
 
 // The working state shared by every call on a device.
-static __device__ __align__(256) unsigned char g_scratch[kLdpNoallocScratchBytes];
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-// Host-side address of g_scratch per device (the symbol name itself is not a
-// device address in host code).
+// Host-side device address of g_scratch, per device, valid for the CUDA
+// context it was looked up in (the symbol name itself is not a device
+// address in host code).  A context created after a cudaDeviceReset loads
+// the module again, at another address, and has another id.
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;
+    void* addr = nullptr;
+};
 std::mutex g_mu;
-void* g_addr[64] = {};
+ScratchAddr g_addr[64];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the calling thread's current context, through the driver entry
+// points the runtime hands out (the library does not link libcuda itself).
+cudaError_t current_ctx_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
+        if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return cudaErrorSymbolNotFound;
+        get_current = (CtxGetCurrentFn)f0;
+        get_id = (CtxGetIdFn)f1;
+    }
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || !c) return cudaErrorDeviceUninitialized;
+    if (get_id(c, id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
 
 size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -58,10 +99,20 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
         set_err(err, errlen, m);
         return LDP_ERR_INVALID;
     }
-    if (o->mode != LDP_MODE_FIXED_STEPS || p->waiting_time || p->n_cg > LDP_MAX_CG || p->freq_save < 1 ||
-        !(p->timestep > 0.0) || !(p->periodic_length > 0.0) || p->number_of_previous_steps) {
-        set_err(err, errlen, "fixed-step runs only, WAITINGTIME off, at most 16 FPTCG entries, positive "
-                             "TIMESTEP and PERIODICLENGTH, FREQSAVE >= 1, no restart (NUMBEROFPREVIOUSSTEPS 0)");
+    const int slots = o->table_slots;
+    if (slots < 16 || slots > LDP_NOALLOC_MAX_SLOTS || (slots & (slots - 1))) {
+        char m[160];
+        std::snprintf(m, sizeof(m), "table_slots = %d; this entry point takes a power of two from 16 to %d",
+                      slots, LDP_NOALLOC_MAX_SLOTS);
+        set_err(err, errlen, m);
+        return LDP_ERR_UNSUPPORTED;
+    }
+    if (o->precision != LDP_PREC_FP64_PLAIN || o->mode != LDP_MODE_FIXED_STEPS || o->event_cap != 0 ||
+        p->waiting_time || p->n_cg > LDP_MAX_CG || p->freq_save < 1 || !(p->timestep > 0.0) ||
+        !(p->periodic_length > 0.0) || p->number_of_previous_steps) {
+        set_err(err, errlen, "FP64 plain fixed-step runs only: no event lists (event_cap 0), WAITINGTIME off, at "
+                             "most 16 FPTCG entries, positive TIMESTEP and PERIODICLENGTH, FREQSAVE >= 1, no "
+                             "restart (NUMBEROFPREVIOUSSTEPS 0)");
         return LDP_ERR_UNSUPPORTED;
     }
     int dev = 0;
@@ -69,25 +120,32 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
         set_err(err, errlen, "no current CUDA device");
         return LDP_ERR_DEVICE;
     }
-    // Set-up, once per device, with that device current: the device address
-    // of the scratch array.
+    // Set-up, once per device and context, with that device current: the
+    // device address of the scratch array.  cudaSetDevice makes the device's
+    // primary context current on this thread (and creates it on first use),
+    // so the context id below is the one the launches run in.
     void* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_addr[dev]) {
+        cudaError_t e = cudaSetDevice(dev);
+        unsigned long long id = 0;
+        if (e == cudaSuccess) e = current_ctx_id(&id);
+        if (e == cudaSuccess && (!g_addr[dev].addr || g_addr[dev].ctx_id != id)) {
             void* a = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&a, g_scratch);
-            if (e != cudaSuccess) {
-                set_err(err, errlen, cudaGetErrorString(e));
-                return LDP_ERR_DEVICE;
+            e = cudaGetSymbolAddress(&a, g_scratch);
+            if (e == cudaSuccess) {
+                g_addr[dev].addr = a;
+                g_addr[dev].ctx_id = id;
             }
-            g_addr[dev] = a;
         }
-        base = g_addr[dev];
+        if (e != cudaSuccess) {
+            set_err(err, errlen, cudaGetErrorString(e));
+            return LDP_ERR_DEVICE;
+        }
+        base = g_addr[dev].addr;
     }
 
     ldp_job_opts opts = *o;
-    opts.table_slots = kSlots;
     opts.tick_cap = 0;
     ldp::KConst k;
     const uint32_t seed = (uint32_t)(p->random_seed < 0 ? 0 : p->random_seed);
@@ -111,14 +169,14 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
     S.state = i32; S.lb = i32 + n; S.bits = i32 + 2 * n; S.state0 = i32 + 3 * n;
     S.cg_last = (double*)take(sizeof(double) * LDP_MAX_CG * n);
     S.cg_well = (int64_t*)take(sizeof(int64_t) * LDP_MAX_CG * n);
-    S.ring_tag = (int64_t*)take(sizeof(int64_t) * kSlots * n);
-    S.ring_data = (int64_t*)take(sizeof(int64_t) * kSlots * n);
+    S.ring_tag = (int64_t*)take(sizeof(int64_t) * slots * n);
+    S.ring_data = (int64_t*)take(sizeof(int64_t) * slots * n);
     S.counts = d_counts;
     S.sums = d_sums;
     S.ticks = nullptr;
     S.fx = d_frames_x;
     S.fv = S.ff = S.fb = S.fpe = S.fke = S.fst = nullptr;
-    if (off > kLdpNoallocScratchBytes) {
+    if (off > kScratchBytes) {
         set_err(err, errlen, "scratch layout exceeds the static array");
         return LDP_ERR_INVALID;
     }
@@ -133,10 +191,16 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
         set_err(err, errlen, cudaGetErrorString((cudaError_t)e));
         return LDP_ERR_DEVICE;
     }
+    // Steps per launch as a job chooses them: o->steps_per_launch, else about
+    // 2^31 trajectory-steps per launch (clamped to 4096 .. 2^24 steps).
+    uint64_t spl = o->steps_per_launch;
+    if (!spl) {
+        spl = (uint64_t)(((int64_t)1 << 31) / std::max<int64_t>(n, 1));
+        spl = std::min<uint64_t>(std::max<uint64_t>(spl, 4096), (uint64_t)1 << 24);
+    }
     const uint64_t nsteps = ldp::effective_steps(*p);
-    const uint64_t spl = 1u << 22;
     for (uint64_t s0 = 1; s0 <= nsteps; s0 += spl) {
-        const uint64_t s1 = (s0 + spl < nsteps + 1) ? s0 + spl : nsteps + 1;
+        const uint64_t s1 = std::min<uint64_t>(s0 + spl, nsteps + 1);
         e = ldp::launch_fp64_steps(k, S, 0, s0, s1, 128, stream);
         if (e) {
             set_err(err, errlen, cudaGetErrorString((cudaError_t)e));
