@@ -18,15 +18,17 @@
 // msd_traj_kernel is the same computation from global memory, used only when
 // one trajectory's frames do not fit in shared memory.
 //
-// msd_smem_f32_kernel: the same for jobs of the FP32 batched path, in FP32:
-// a trajectory's frames are staged as offsets from its first frame, rounded
-// to FP32 (an error of at most 2^-24 of the offset), and the squares are
-// summed in FP32 (32-way interleaved partials of ~nframe/32 terms each).
-// Half the shared-memory bytes per term, which bound the FP64 kernel; with
-// 8 lags per item, a loop without per-term tests over the origins all of
-// them have, and four blocks per SM (54 KiB each) to hide the shared-load
-// latency.  The FP64 plain path keeps the FP64 kernel (bit-identical to
-// the oracle).
+// msd_smem_f32_kernel: the same for jobs of the FP32 batched path: a
+// trajectory's frames are staged in shared memory as offsets from its first
+// frame, rounded to FP32 (an error of at most 2^-24 of the offset), the
+// displacement x[k + lag] - x[k] is taken in FP32, and its square is formed
+// and accumulated in FP64 (widened displacement, fma into FP64 32-way
+// interleaved partials of ~nframe/32 terms each), so the moment sums are
+// FP64 as on the FP64 path.  Half the shared-memory bytes per term, which
+// bound the FP64 kernel; with 6 lags per item, a loop without per-term
+// tests over the origins all of them have, and four blocks per SM (54 KiB
+// each) to hide the shared-load latency.  The FP64 plain path keeps the
+// FP64 kernel (bit-identical to the oracle).
 //
 // msd_reduce_kernel: one block per lag sums msd0 over trajectories with
 // Kahan compensation in a fixed order (per-thread strided partials, then a
@@ -42,7 +44,7 @@ constexpr int kMsdSmemBytes = 100 * 1024;   // two blocks per SM
 constexpr int kMsdBlock = 256;
 constexpr int kMsdLags = 4;                  // lags per work item (x[k] reuse)
 constexpr int kMsdF32SmemBytes = 54 * 1024;  // FP32 kernel: four blocks per SM
-// Lean FP32 instance (msd_smem_f32_kernel<128, 4, 16, true>), for
+// Lean FP32 instance (msd_smem_f32_kernel<128, 2, 16, true>), for
 // post-processing that runs beside the persistent FP32 kernel: one warp per
 // SMSP at 32 registers is what three persistent blocks leave of an SM's
 // register file, and one staged trajectory (12 KB at 3001 frames) fits in
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(kBlk, kMinB) msd_smem_f32_kernel(const double*
         const int g0 = (it - j * ngroup) * kNL;
         const float* x = fs32 + j * nframe;
         int lag[kNL], cnt[kNL];
-        float acc[kNL];
+        double acc[kNL];
         // Slots past the last lag repeat the group's first lag (results not
         // written), so that kmin is the shortest origin count of real lags.
         const int lag0 = (int)lags[g0];
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(kBlk, kMinB) msd_smem_f32_kernel(const double*
             if (cnt[r] < 0) cnt[r] = 0;
             kmin = cnt[r] < kmin ? cnt[r] : kmin;
             kmax = cnt[r] > kmax ? cnt[r] : kmax;
-            acc[r] = 0.0f;
+            acc[r] = 0.0;
         }
         // Origins every lag of the item has: no per-term test.
         int k = lane;
@@ -149,8 +151,8 @@ __global__ void __launch_bounds__(kBlk, kMinB) msd_smem_f32_kernel(const double*
             const float xk = x[k];
 #pragma unroll
             for (int r = 0; r < kNL; ++r) {
-                const float d = x[k + lag[r]] - xk;
-                acc[r] = fmaf(d, d, acc[r]);
+                const double d = (double)(x[k + lag[r]] - xk);
+                acc[r] = fma(d, d, acc[r]);
             }
         }
         for (; k < kmax; k += 32) {
@@ -158,18 +160,18 @@ __global__ void __launch_bounds__(kBlk, kMinB) msd_smem_f32_kernel(const double*
 #pragma unroll
             for (int r = 0; r < kNL; ++r) {
                 if (k < cnt[r]) {
-                    const float d = x[k + lag[r]] - xk;
-                    acc[r] = fmaf(d, d, acc[r]);
+                    const double d = (double)(x[k + lag[r]] - xk);
+                    acc[r] = fma(d, d, acc[r]);
                 }
             }
         }
 #pragma unroll
         for (int r = 0; r < kNL; ++r) {
-            float v = acc[r];
+            double v = acc[r];
 #pragma unroll
             for (int h = 16; h >= 1; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
             const int i = g0 + r;
-            if (lane == 0 && i < nlag) msd0[(int64_t)i * ntraj + t0 + j] = cnt[r] > 0 ? (double)v / (double)cnt[r] : 0.0;
+            if (lane == 0 && i < nlag) msd0[(int64_t)i * ntraj + t0 + j] = cnt[r] > 0 ? v / (double)cnt[r] : 0.0;
         }
     }
 }
@@ -273,12 +275,12 @@ int launch_msd(const double* frames, int64_t nframe, int64_t ntraj, const int64_
         const size_t smem = (size_t)G * (size_t)per_traj;
         const int64_t nblk = (ntraj + G - 1) / G;
         if (lean) {
-            auto* kern = msd_smem_f32_kernel<128, 4, 16, true>;
+            auto* kern = msd_smem_f32_kernel<128, 2, 16, true>;
             e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return (int)e;
             kern<<<(unsigned)nblk, 128, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag, msd0);
         } else if (f32) {
-            auto* kern = msd_smem_f32_kernel<kMsdBlock, 8, 4, false>;
+            auto* kern = msd_smem_f32_kernel<kMsdBlock, 6, 4, false>;
             e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return (int)e;
             kern<<<(unsigned)nblk, kMsdBlock, smem, s>>>(frames, (int)nframe, ntraj, G, lags, (int)nlag, msd0);

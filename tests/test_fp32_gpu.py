@@ -161,41 +161,12 @@ def test_fp32_first_passage_refill_independent_of_shape():
     assert np.all((c[L.C_FPT2] == 1) ^ ((c[L.C_FLAGS] & L.FLAG_CENSORED) != 0))
 
 
-def pooled(r, ci, si):
-    c = r["counts"][ci].sum()
-    return r["sums"][si].sum() / max(c, 1), c
-
-
-def test_fp32_statistics_agree_with_fp64(ctx):
-    # 65536 trajectories x 4e5 steps of the quick_test model (dt 1e-4), both
-    # precisions on the same noise.  Mean event times (MFPT, MFPT2, MTPT)
-    # agree within max(1%, 3 standard errors of the difference), the state
-    # fractions within 1e-3, the MSD within 2% at lags with > 100 origins.
-    p = quick(steps=400_000, freq=100)
-    a = run(ctx, p, ldp.PREC_FP64_PLAIN, lanes=65536)
-    b = run(ctx, p, ldp.PREC_FP32_BATCHED, lanes=65536)
-    for ci, si in ((L.C_FPT, L.S_FPT), (L.C_FPT2, L.S_FPT2), (L.C_TPT, L.S_TPT)):
-        ma, na = pooled(a, ci, si)
-        mb, nb = pooled(b, ci, si)
-        assert na > 10000 and nb > 10000
-        se = np.sqrt(ma * ma / na + mb * mb / nb)
-        print(f"field {ci}: fp64 {ma:.5f} ({na}) fp32 {mb:.5f} ({nb}) rel diff {(mb - ma) / ma:+.4%}")
-        assert abs(mb - ma) < max(0.01 * ma, 3 * se), (ci, ma, mb, se)
-    fa = a["counts"][L.C_STATE1].sum() / (a["counts"][L.C_STATE0].sum() + a["counts"][L.C_STATE1].sum())
-    fb = b["counts"][L.C_STATE1].sum() / (b["counts"][L.C_STATE0].sum() + b["counts"][L.C_STATE1].sum())
-    assert abs(fa - fb) < 1e-3
-    nf = p.number_of_steps // p.freq_save + 1
-    ok = (nf - a["lags"]) > 100
-    ok[0] = False
-    np.testing.assert_allclose(b["msd"][ok], a["msd"][ok], rtol=0.02)
-
-
 def test_fp32_msd_matches_an_fp64_msd_of_its_own_frames(ctx):
     # The FP32 path's MSD kernel stages each trajectory's frames as FP32
-    # offsets from its first frame and sums the squares in FP32.  Against an
-    # FP64 brute-force MSD of the same saved frames, every per-trajectory
-    # value is within 1e-5 relative (staging rounding ~1e-7, FP32 partial
-    # sums of <= 94 terms ~1e-6).
+    # offsets from its first frame, takes displacements in FP32 and sums
+    # their squares in FP64.  Against an FP64 brute-force MSD of the same
+    # saved frames, every per-trajectory value is within 1e-6 relative (the
+    # staging and displacement roundings, ~1e-7).
     p = quick(steps=120_000, freq=40)
     with ldp.Job(ctx, p, precision=ldp.PREC_FP32_BATCHED, lanes=500) as job:
         job.run()
@@ -205,8 +176,8 @@ def test_fp32_msd_matches_an_fp64_msd_of_its_own_frames(ctx):
     assert fx.shape == (3001, 500) and len(lags) > 20
     nf = fx.shape[0]
     want = np.stack([((fx[L:] - fx[:nf - L]) ** 2).mean(0) for L in lags])
-    np.testing.assert_allclose(m0, want, rtol=1e-5)
-    np.testing.assert_allclose(msd, want.mean(1), rtol=1e-5)
+    np.testing.assert_allclose(m0, want, rtol=1e-6)
+    np.testing.assert_allclose(msd, want.mean(1), rtol=1e-6)
 
 
 def test_fp32_first_passage_distribution_matches_fp64(ctx):
