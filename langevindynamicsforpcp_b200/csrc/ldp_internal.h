@@ -14,6 +14,7 @@ struct Fp32Runtime;
 }
 
 constexpr int kCtxMarks = 16;
+constexpr int kCtxF64Streams = 2;   // streams FP64 plain jobs of a batch share
 
 struct ldp_ctx {
     cudaEvent_t marks[kCtxMarks] = {};   // ldp_ctx_mark / ldp_ctx_elapsed_ms
@@ -32,6 +33,10 @@ struct ldp_ctx {
     cudaStream_t rd = nullptr;     // result reads of finished jobs, beside running work
     cudaStream_t gside = nullptr;  // side branch captured into batch graphs
     cudaEvent_t gjoin = nullptr;   // joins that branch back before the capture ends
+    // FP64 plain jobs of a batch: forked from `stream`, joined back to it.
+    cudaStream_t f64s[kCtxF64Streams] = {};
+    cudaEvent_t f64j[kCtxF64Streams] = {};
+    cudaEvent_t f64fork = nullptr;
 };
 
 struct ldp_job {

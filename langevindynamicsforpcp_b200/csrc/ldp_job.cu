@@ -102,6 +102,14 @@ extern "C" void ldp_destroy(ldp_ctx* ctx) {
             cudaStreamSynchronize(*x);
             cudaStreamDestroy(*x);
         }
+    for (int k = 0; k < kCtxF64Streams; ++k) {
+        if (ctx->f64s[k]) {
+            cudaStreamSynchronize(ctx->f64s[k]);
+            cudaStreamDestroy(ctx->f64s[k]);
+        }
+        if (ctx->f64j[k]) cudaEventDestroy(ctx->f64j[k]);
+    }
+    if (ctx->f64fork) cudaEventDestroy(ctx->f64fork);
     if (ctx->gjoin) cudaEventDestroy(ctx->gjoin);
     fp32_destroy_runtime(ctx);
     for (int i = 0; i < kCtxMarks; ++i)
@@ -480,14 +488,15 @@ static uint64_t auto_steps_per_launch(const ldp_job* job) {
     return s;
 }
 
-extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
+// Enqueues a job's work on stream s (the context's stream, or for FP64
+// plain jobs of a batch one of the context's FP64 batch streams).
+static ldp_status submit_on(ldp_ctx* ctx, ldp_job* job, cudaStream_t s) {
     if (!ctx || !job) return LDP_ERR_INVALID;
     if (job->submitted) {
         ldp_set_error(ctx, "job already submitted");
         return LDP_ERR_INVALID;
     }
     CUDA_OR_FAIL(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = ctx->stream;
     if (!job->arena && job_arena(job, true) == 0) {
         ldp_set_error(ctx, "cudaMalloc of %zu bytes failed", job_arena(job, false));
         return LDP_ERR_NOMEM;
@@ -547,6 +556,11 @@ extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
     }
     CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[2], s));
     return LDP_OK;
+}
+
+extern "C" ldp_status ldp_submit(ldp_ctx* ctx, ldp_job* job) {
+    if (!ctx) return LDP_ERR_INVALID;
+    return submit_on(ctx, job, ctx->stream);
 }
 
 // FP32 batched jobs advance in rounds: when the launches enqueued so far
@@ -793,8 +807,8 @@ extern "C" ldp_status ldp_job_msd_traj(ldp_job* job, double* msd0) {
 }
 
 // Registers every FP32 batched job of the list before enqueueing any launch,
-// so that all of them share each persistent launch; FP64 plain jobs are
-// submitted one after the other.
+// so that all of them share each persistent launch; FP64 plain jobs run
+// side by side on two streams forked from the context's stream.
 extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) {
     if (!ctx || (!jobs && njobs) || njobs < 0) return LDP_ERR_INVALID;
     CUDA_OR_FAIL(ctx, cudaSetDevice(ctx->device));
@@ -806,11 +820,42 @@ extern "C" ldp_status ldp_submit_batch(ldp_ctx* ctx, ldp_job** jobs, int njobs) 
             return LDP_ERR_INVALID;
         }
     }
-    for (int i = 0; i < njobs; ++i)
-        if (jobs[i]->o.precision != LDP_PREC_FP32_BATCHED) {
-            ldp_status st = ldp_submit(ctx, jobs[i]);
-            if (st != LDP_OK) return st;
+    // FP64 plain jobs: one alone runs on the context's stream.  Several run
+    // side by side on the context's FP64 batch streams, forked from and
+    // joined back to the context's stream: a job smaller than a wave of
+    // resident blocks (65536 trajectories are 512 blocks of 128 threads,
+    // 86 % of the 592 slots of 148 SMs) leaves the rest of the GPU to the
+    // next job instead of idling until it drains.
+    int n64 = 0;
+    for (int i = 0; i < njobs; ++i) n64 += jobs[i]->o.precision != LDP_PREC_FP32_BATCHED;
+    if (n64 == 1) {
+        for (int i = 0; i < njobs; ++i)
+            if (jobs[i]->o.precision != LDP_PREC_FP32_BATCHED) {
+                ldp_status st = submit_on(ctx, jobs[i], s);
+                if (st != LDP_OK) return st;
+            }
+    } else if (n64 > 1) {
+        if (!ctx->f64s[0]) {
+            for (int k = 0; k < kCtxF64Streams; ++k) {
+                CUDA_OR_FAIL(ctx, cudaStreamCreateWithFlags(&ctx->f64s[k], cudaStreamNonBlocking));
+                CUDA_OR_FAIL(ctx, cudaEventCreateWithFlags(&ctx->f64j[k], cudaEventDisableTiming));
+            }
+            CUDA_OR_FAIL(ctx, cudaEventCreateWithFlags(&ctx->f64fork, cudaEventDisableTiming));
         }
+        CUDA_OR_FAIL(ctx, cudaEventRecord(ctx->f64fork, s));
+        for (int k = 0; k < kCtxF64Streams; ++k) CUDA_OR_FAIL(ctx, cudaStreamWaitEvent(ctx->f64s[k], ctx->f64fork, 0));
+        int k = 0;
+        for (int i = 0; i < njobs; ++i)
+            if (jobs[i]->o.precision != LDP_PREC_FP32_BATCHED) {
+                ldp_status st = submit_on(ctx, jobs[i], ctx->f64s[k]);
+                if (st != LDP_OK) return st;
+                k = (k + 1) % kCtxF64Streams;
+            }
+        for (int k2 = 0; k2 < kCtxF64Streams; ++k2) {
+            CUDA_OR_FAIL(ctx, cudaEventRecord(ctx->f64j[k2], ctx->f64s[k2]));
+            CUDA_OR_FAIL(ctx, cudaStreamWaitEvent(s, ctx->f64j[k2], 0));
+        }
+    }
     int launches[4] = {0, 0, 0, 0};
     ldp_job* first[4] = {nullptr, nullptr, nullptr, nullptr};
     // A type whose queue holds no unfinished job gets each job's
