@@ -165,3 +165,28 @@ def test_job_id_and_seed_select_streams(ctx):
     c, _, _ = run_both(ctx, p, seed=2, job_id=0)
     assert not np.array_equal(a["x_final"], b["x_final"])
     assert not np.array_equal(a["x_final"], c["x_final"])
+
+
+def test_fp64_batch_jobs_side_by_side_equal_each_alone(ctx):
+    # A batch runs its FP64 plain jobs on two streams at once; each job's
+    # results equal the same job run alone, bit for bit, and its MSD too.
+    ps = [quick(steps=40_000, freq=20), quick(steps=60_000, freq=20, tau=1e-3), double(steps=40_000, freq=20)]
+    for p in ps:
+        p.random_seed = 1234
+    lanes = [600, 300, 900]
+    jobs = [ldp.Job(ctx, p, lanes=n, job_id=i) for i, (p, n) in enumerate(zip(ps, lanes))]
+    ldp.submit_batch(ctx, jobs)
+    got = []
+    for j in jobs:
+        j.wait()
+        r = j.results()
+        r["lags"], r["msd"] = j.msd()
+        got.append(r)
+        j.close()
+    for i, (p, n) in enumerate(zip(ps, lanes)):
+        with ldp.Job(ctx, p, lanes=n, job_id=i) as job:
+            job.run()
+            alone = job.results()
+            alone["lags"], alone["msd"] = job.msd()
+        for k in ("counts", "sums", "x_final", "frames_x", "msd"):
+            np.testing.assert_array_equal(got[i][k], alone[k], err_msg=f"job {i} {k}")
