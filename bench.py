@@ -41,6 +41,13 @@ OPS_PER_STEP = 70   # lane instructions per overdamped single-barrier step (algo
 # four steps, two Box-Muller pairs (14 each), update 3, tests 3.
 OPS_PER_STEP_AS_BUILT = (58 + 2 * 14) / 4 + 3 + 3
 NJOBS, NTRAJ, NSTEPS, FREQSAVE = 16, 65536, 300000, 100
+FP64_STEPS = 2      # timed passes of the FP64 plain leg (one untimed before)
+# Accuracy leg: the mix's most event-rich job (index 14: H_low 2, flip rate
+# 4.84) with 65536 trajectories x 5e6 steps (50 time units), both precisions
+# on the same noise: ~3 first passages per trajectory, ~2e5 events, so the
+# FP64 mean's relative standard error is ~0.2 %.  Its device times also give
+# both paths' throughput on an event-heavy workload.
+ACC_JOB, ACC_NTRAJ, ACC_NSTEPS, ACC_FREQSAVE = 14, 65536, 5_000_000, 2500
 # DRAM bytes per particle-step of the persistent kernel: 0.0873 B measured by
 # ncu with frames every 100 steps, of which the frames are 8 B per frame
 # (0.0801 B per step); the rest (0.0072 B: retire records, ring) is kept and
@@ -134,35 +141,67 @@ def run_batch(ldp, ctx, params, precision, job_id0=0):
 
 
 def job_summary(job):
-    """MSD curve and renewal-event means of a finished job (host copies)."""
+    """MSD curve, pooled renewal-event means with their standard errors, and
+    the state-1 fraction of a finished job (host copies)."""
     from langevindynamicsforpcp_b200 import _lib as L
     r = job.results(frames=False, ticks=False)
     lags, msd = job.msd()
     c, s = r["counts"], r["sums"]
-    out = {"msd": msd, "lags": lags}
-    for name, ci, si in (("fpt", L.C_FPT, L.S_FPT), ("fpt2", L.C_FPT2, L.S_FPT2), ("tpt", L.C_TPT, L.S_TPT)):
+    out = {"msd": msd, "lags": lags, "ntraj": c.shape[1]}
+    for name, ci, si in (("fpt", L.C_FPT, L.S_FPT), ("fpt2", L.C_FPT2, L.S_FPT2), ("tpt", L.C_TPT, L.S_TPT),
+                         ("tpt2", L.C_TPT2, L.S_TPT2), ("fptcg2", L.C_CG0, L.S_CG0)):
         n = float(c[ci].sum())
-        per = np.where(c[ci] > 0, s[si] / np.maximum(c[ci], 1), np.nan)
-        out[name] = (float(s[si].sum()) / n if n else None, int(n),
-                     float(np.nanstd(per) / np.sqrt(np.sum(c[ci] > 0))) if n else None)
+        if n == 0:
+            out[name] = (None, 0, None)
+            continue
+        mean = float(s[si].sum()) / n
+        # standard error of the pooled ratio estimator over trajectories
+        resid = s[si] - mean * c[ci]
+        out[name] = (mean, int(n), float(np.sqrt((resid ** 2).sum()) / n))
+    s0, s1 = float(c[L.C_STATE0].sum()), float(c[L.C_STATE1].sum())
+    out["state1_fraction"] = s1 / (s0 + s1)
     return out
 
 
 def compare_summaries(a, b):
-    """FP32 batched job 0 against the FP64 plain run of the same job (same
-    parameters, seed and job id): relative differences, with the standard
-    error of the FP64 mean for scale (the two runs share their noise but
-    not every trajectory, so the difference includes sampling noise)."""
+    """FP32 batched against the FP64 plain run of the same job (same
+    parameters, seed, job id and noise): relative differences, with the
+    relative standard error of the FP64 estimate for scale."""
     out = {}
-    ok = b["msd"] > 0
+    ok = (b["lags"] > 0) & (b["msd"] > 0)
     rel = np.abs(a["msd"][ok] - b["msd"][ok]) / b["msd"][ok]
     out["msd_max_rel_err"] = float(rel.max())
     out["msd_mean_rel_err"] = float(rel.mean())
-    for k in ("fpt", "fpt2", "tpt"):
+    for k in ("fpt", "fpt2", "tpt", "tpt2", "fptcg2"):
         (ma, na, _), (mb, nb, se) = a[k], b[k]
         if ma is not None and mb is not None:
-            out[k] = {"fp32_mean": ma, "fp64_mean": mb, "rel_err": abs(ma - mb) / mb, "fp64_rel_se": se / mb if se else None,
-                      "events_fp32": na, "events_fp64": nb}
+            out[k] = {"fp32_mean": ma, "fp64_mean": mb, "rel_err": abs(ma - mb) / mb,
+                      "fp64_rel_se": se / mb if se else None, "events_fp32": na, "events_fp64": nb,
+                      "events_per_traj": nb / b["ntraj"]}
+    fa, fb = a["state1_fraction"], b["state1_fraction"]
+    out["state1_fraction"] = {"fp32": fa, "fp64": fb, "rel_err": abs(fa - fb) / fb}
+    return out
+
+
+def accuracy_leg(ldp, ctx, job_id0):
+    """FP32 batched vs FP64 plain on one job of the mix, sized for a small
+    FP64 standard error (outside the timed region; each run's device time is
+    reported as an event-heavy throughput figure)."""
+    p = workload_params(ldp, ACC_JOB, 1, nsteps=ACC_NSTEPS, freqsave=ACC_FREQSAVE)[0]
+    sums, rate = {}, {}
+    for prec in (ldp.PREC_FP32_BATCHED, ldp.PREC_FP64_PLAIN):
+        with ldp.Job(ctx, p, lanes=ACC_NTRAJ, precision=prec, job_id=job_id0 + ACC_JOB) as j:
+            j.run()
+            sums[prec] = job_summary(j)
+            t = j.timing()
+            rate[prec] = ACC_NTRAJ * ACC_NSTEPS / ((t["integrate_ms"] + t["msd_ms"]) * 1e-3)
+    out = compare_summaries(sums[ldp.PREC_FP32_BATCHED], sums[ldp.PREC_FP64_PLAIN])
+    out["sample"] = (f"job {ACC_JOB} of the mix (H_low 2, flip rate 4.84), {ACC_NTRAJ} trajectories x "
+                     f"{ACC_NSTEPS} steps, both precisions on the same noise")
+    out["event_heavy_throughput"] = {
+        "fp32": rate[ldp.PREC_FP32_BATCHED], "fp64": rate[ldp.PREC_FP64_PLAIN],
+        "ratio": rate[ldp.PREC_FP32_BATCHED] / rate[ldp.PREC_FP64_PLAIN], "unit": "particle-steps/s",
+        "fpt_events_per_traj": out.get("fpt", {}).get("events_per_traj")}
     return out
 
 
@@ -267,7 +306,6 @@ def main():
             kernel_ms.append(max(j.timing()["integrate_ms"] for j in jobs))
             msd_ms.append(times[-1] - kernel_ms[-1])
             launches += sum(j.timing()["launches"] for j in jobs)
-            acc32 = job_summary(jobs[0])
             for j in jobs:
                 j.close()
     clocks = clk.summary()
@@ -275,20 +313,27 @@ def main():
     value = psteps * world / (step_ms * 1e-3)
     shape_used = _tune.get_fp32_shape(ctx)
 
-    # ---- FP64 plain leg (one job, 1/16 of the work) for the ratio ----
+    # ---- FP64 plain leg: the same 16 jobs (2^20 trajectories), one batch ----
+    # (the batch runs the FP64 jobs side by side on two streams); one
+    # untimed pass, then FP64_STEPS timed passes.
     t64 = []
-    for it in range(args.warmup + args.steps):
-        with ldp.Job(ctx, params[0], lanes=NTRAJ, precision=ldp.PREC_FP64_PLAIN, job_id=job_id0) as j:
-            barrier()
-            ctx.mark(2)
-            j.submit()
+    for it in range(1 + FP64_STEPS):
+        jobs64 = [ldp.Job(ctx, p, lanes=NTRAJ, precision=ldp.PREC_FP64_PLAIN, job_id=job_id0 + i)
+                  for i, p in enumerate(params)]
+        flush_l2()
+        barrier()
+        ctx.mark(2)
+        ldp.submit_batch(ctx, jobs64)
+        for j in jobs64:
             j.wait()
-            ctx.mark(3)
-            if it >= args.warmup:
-                t64.append(ctx.elapsed_ms(2, 3))
-            acc64 = job_summary(j)
-    fp64_value = NTRAJ * NSTEPS / (sum(t64) / len(t64) * 1e-3)
-    accuracy = compare_summaries(acc32, acc64)
+        ctx.mark(3)
+        if it >= 1:
+            t64.append(ctx.elapsed_ms(2, 3))
+        for j in jobs64:
+            j.close()
+    fp64_ms = rep.max_over_ranks(sum(t64) / len(t64))
+    fp64_value = psteps / (fp64_ms * 1e-3)
+    accuracy = accuracy_leg(ldp, ctx, job_id0)
 
     # ---- end to end through the C ABI: host params in, host results out ----
     e2e_t = []
@@ -325,7 +370,12 @@ def main():
             peaks = json.load(f)
     props = torch.cuda.get_device_properties(local)
     sms = props.multi_processor_count
-    fmax = peaks.get("sm_max_mhz", 1965.0)
+    if peaks.get("sm_max_mhz"):
+        fmax = float(peaks["sm_max_mhz"])
+        fsrc = "sm_max_mhz of the measured peaks file"
+    else:
+        fmax = float(clocks.get("sm_max_mhz") or 1965.0)
+        fsrc = "clocks.max.sm sampled by nvidia-smi during the timed region (no measured peaks file)"
     peak_issue = sms * 4 * 32 * fmax * 1e6 / 1e9            # Glane-instr/s at the max clock
     kms = sum(kernel_ms) / len(kernel_ms)
     achieved = psteps * OPS_PER_STEP / (kms * 1e-3) / 1e9
@@ -333,14 +383,15 @@ def main():
     roofline = {"bound": "issue", "achieved": achieved, "peak": peak_issue, "unit": "Ginstr/s",
                 "frac": achieved / peak_issue, "traffic": DRAM_BYTES_PER_STEP * psteps,
                 "traffic_scope": "DRAM bytes of the persistent kernel per bench step (all its launches): "
-                                 f"{DRAM_BYTES_PER_STEP} B per particle-step from the ncu capture in "
-                                 "profiles/fp32_persistent_kernel__single_over_113664traj_120000steps.md, "
-                                 "scaled by particle-steps and frame interval; algorithmic bytes: the frames, 8 B per FREQSAVE steps",
+                                 f"{DRAM_BYTES_PER_STEP} B per particle-step, from an ncu capture of the kernel "
+                                 "on 113664 trajectories x 120000 steps with frames every 100 steps, the frame "
+                                 "part scaled to this workload's frame interval; algorithmic bytes: the frames, "
+                                 "8 B per FREQSAVE steps",
                 "kernel": "fp32_persistent_kernel<single, overdamped>",
                 "ops_per_step": OPS_PER_STEP, "kernel_ms": kms,
                 "ops_per_step_as_built": OPS_PER_STEP_AS_BUILT,
                 "frac_as_built": psteps * OPS_PER_STEP_AS_BUILT / (kms * 1e-3) / 1e9 / peak_issue,
-                "peak_basis": f"{sms} SMs x 128 lanes x sm_max_mhz {fmax:g} (MEASURED_PEAKS.json)",
+                "peak_basis": f"{sms} SMs x 128 lanes x {fmax:g} MHz ({fsrc})",
                 "frac_at_sampled_clock": achieved / (sms * 128 * fclk * 1e6 / 1e9)}
 
     if rank == 0:
@@ -350,9 +401,10 @@ def main():
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(workload_config(world), fp32_shape=shape_used, tuned=bool(shape)),
-            "fp64_plain": {"value": fp64_value, "unit": "particle-steps/s",
-                           "sample": f"job 0 alone ({NTRAJ} trajectories x {NSTEPS} steps)"},
-            "fp32_over_fp64": value / world / fp64_value,
+            "fp64_plain": {"value": fp64_value * world, "unit": "particle-steps/s", "ms_per_step": fp64_ms,
+                           "sample": f"the same {NJOBS} jobs x {NTRAJ} trajectories x {NSTEPS} steps in one batch "
+                                     f"(FP64 jobs side by side on two streams), {FP64_STEPS} timed passes"},
+            "fp32_over_fp64": value / (fp64_value * world),
             "accuracy_vs_fp64": accuracy,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
