@@ -55,14 +55,21 @@ ACC_JOB, ACC_NTRAJ, ACC_NSTEPS, ACC_FREQSAVE = 14, 65536, 5_000_000, 2500
 DRAM_BYTES_PER_STEP = 0.0072 + 8.0 / FREQSAVE
 
 
-def workload_params(ldp, job0=0, njobs=NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE):
-    base = os.path.join(ROOT, "tests", "golden", "inp", "CuIDB_single__2.0_7.2_m1.0_1.00e-05.inp")
+BASE_INP = os.path.join(ROOT, "tests", "golden", "inp", "CuIDB_single__2.0_7.2_m1.0_1.00e-05.inp")
+
+
+def job_draws():
+    """(H_low, flip rate) of the 64 jobs the mix cycles through."""
     rng = np.random.default_rng(1234)
-    draws = [(float(rng.choice([2.0, 3.0, 4.0, 5.0])), float(10 ** rng.uniform(-2, 2))) for _ in range(64)]
+    return [(float(rng.choice([2.0, 3.0, 4.0, 5.0])), float(10 ** rng.uniform(-2, 2))) for _ in range(64)]
+
+
+def workload_params(ldp, job0=0, njobs=NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE):
+    draws = job_draws()
     out = []
     for j in range(job0, job0 + njobs):
         h, k = draws[j % 64]
-        p = ldp.params_from_inp(base)
+        p = ldp.params_from_inp(BASE_INP)
         p.overdamped, p.timestep, p.tau = 1, 1e-5, 1.0 / k
         p.barrier_heights[0][0], p.barrier_heights[0][1] = 3.6 * h, h
         p.number_of_steps, p.freq_save = nsteps, freqsave
@@ -70,6 +77,55 @@ def workload_params(ldp, job0=0, njobs=NJOBS, nsteps=NSTEPS, freqsave=FREQSAVE):
         p.random_seed = 1234
         out.append(p)
     return out
+
+
+def reference_inps(nproc, trials):
+    """.inp files of the mix for the reference's executable, one per
+    process: process i runs job i mod 16 (same model, parameters, step count
+    and frame interval as the device jobs) with `trials` trials of its SIMD
+    lanes and its own RANDOMSEED."""
+    draws = job_draws()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    out = []
+    for i in range(nproc):
+        h, k = draws[i % NJOBS]
+        out.append(refrun.inp_text(BASE_INP, {
+            "OUTPUTBASE": "b", "OVERDAMPED": "true", "TIMESTEP": "1e-05", "TAU": repr(1.0 / k),
+            "BARRIERHEIGHTS": f"{3.6 * h!r} {h!r}", "NUMBEROFSTEPS": str(NSTEPS), "NUMBEROFPREVIOUSSTEPS": "0",
+            "NUMBEROFRUNS": str(trials), "FREQSAVE": str(FREQSAVE), "WAITINGTIME": "false", "WRITEX": "false",
+            "READRESTART": "false", "WRITERESTART": "false", "RANDOMSEED": str(1234 + i), "PRINTTIMER": "false"}))
+    return out
+
+
+# Trials per process in one round of the reference arm: 32 x 8 lanes x
+# 300000 steps is about 3 s per core at the AVX-512 build's ~2.5e7
+# particle-steps/s.
+REF_TRIALS = 32
+
+
+def reference_round(trials=REF_TRIALS):
+    """One round of the reference's own code (oracle/_ref, AVX-512 build) on
+    every host core: one single-rank process per core, all started together;
+    particle-steps over the wall time of the slowest.  None when the build
+    is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    if not refrun.available("single"):
+        return None
+    cores = os.cpu_count() or 1
+    lanes = refrun.lanes(True)
+    with refrun.Runs(refrun.exe("single"), reference_inps(cores, trials)) as r:
+        if not r.ok():
+            raise RuntimeError("reference executable failed: " + next(e for e, c in zip(r.errors, r.returncodes)
+                                                                     if c != 0))
+        wall = r.wall_s
+    steps = cores * trials * lanes * NSTEPS
+    return {"value": steps / wall, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{cores} single-rank processes of the reference's AVX-512 build (oracle/_ref, GCC, "
+                      f"MPI and MKL-VSL stand-ins), process i on job i mod {NJOBS} of the mix: {trials} trials x "
+                      f"{lanes} lanes x {NSTEPS} steps each, {FREQSAVE}-step frames, all statistics as the device "
+                      f"jobs; wall time of the slowest process"}
 
 
 class ClockSampler:
@@ -216,9 +272,10 @@ def cpu_baseline_worker(args):
     return ntraj * nsteps, time.perf_counter() - t
 
 
-def cpu_baseline(budget_s=12.0):
+def cpu_baseline_port():
     """The CPU oracle (scalar C port of the reference's per-step algorithm)
-    on every host core for a bounded sample of job 0."""
+    on every host core for a bounded sample of job 0: the stand-in when the
+    reference's own build is absent."""
     cores = os.cpu_count() or 1
     nsteps = 200_000
     ntraj = 8          # trajectories per worker; ~6e6 steps/s per core
@@ -229,6 +286,12 @@ def cpu_baseline(budget_s=12.0):
     wall = max(r[1] for r in res)
     return {"value": steps / wall, "unit": "particle-steps/s", "cores": cores, "kind": "port",
             "sample": f"{cores} processes x {ntraj} trajectories x {nsteps} steps of job 0 (oracle/ldp_oracle.c)"}
+
+
+def cpu_baseline():
+    """The reference's CPU path timed on the host cores (one round of its own
+    build), else the oracle port."""
+    return reference_round() or cpu_baseline_port()
 
 
 def main():
@@ -443,11 +506,12 @@ def C_sizeof_params():
 
 def bench_reference(args, rank, world):
     """The reference's CPU path for this workload on the host cores: the
-    reference build in oracle/_ref when present, else the CPU oracle port."""
+    reference's own build in oracle/_ref (one process per core, each round a
+    bounded sample of the mix), else the CPU oracle port.  Rank 0 alone runs
+    it; the product library is not loaded."""
     if rank != 0:
         return
-    vals = []
-    kind = "port"
+    vals, r = [], None
     for it in range(args.warmup + args.steps):
         r = cpu_baseline()
         if it >= args.warmup:
@@ -457,7 +521,7 @@ def bench_reference(args, rank, world):
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(world),
-            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": kind,
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

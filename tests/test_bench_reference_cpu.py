@@ -1,7 +1,8 @@
-"""bench.py's reference arm (the oracle port on the host cores) runs on the
-CPU; its JSON line keeps the contract the GPU arm keeps: the same metric,
-unit and workload description, the sample it timed, and an end-to-end
-entry with no host-device traffic."""
+"""bench.py's reference arm (the reference's own build in oracle/_ref on the
+host cores, else the oracle port) runs on the CPU; its JSON line keeps the
+contract the GPU arm keeps: the same metric, unit and workload description,
+the sample it timed, and an end-to-end entry with no host-device traffic.
+The arm never loads the product library."""
 import json
 import os
 import subprocess
@@ -27,3 +28,16 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_runs_the_reference_build_without_the_product_library():
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0'];"
+            "runpy.run_path('bench.py', run_name='__main__');"
+            "print('MAPPED', any('libldp' in l for l in open('/proc/self/maps')))")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "MAPPED False" in r.stdout
+    d = json.loads(next(l for l in r.stdout.splitlines() if l.startswith("{")))
+    if os.access(os.path.join(ROOT, "oracle", "_ref", "langevinDynamicsSingleBarrier"), os.X_OK):
+        assert d["cpu_baseline"]["kind"] == "reference"
+        assert "AVX-512" in d["cpu_baseline"]["sample"]
