@@ -617,6 +617,117 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     if (finish) retire(s, vk, 0);
 }
 
+// The light step: the commonest special steps, handled in the hot loop
+// with the same result the general step gives them, so that the warp does
+// not pay for the out-of-line call.  Returns 0 when the step needs the
+// general step; 1 when it was handled and the countdown is unchanged; 2 when
+// it was handled and *lrel holds the steps from s to the next special step.
+//  * A frame step (the countdown ends at a frame, not at a flip or the last
+//    step), the position inside its band, no WRITEX series: the frame is
+//    written (FP64 cell * L + xp) and the countdown restarts.
+//  * A band exit inside the cell (a barrier flank entered or left), with no
+//    change of well (barrier top) or local barrier: new band and force.
+//  * A crossing of the cell edge into the flat band of the neighbour cell
+//    whose barrier is the cached one (the cell left last) and has not passed
+//    its pending flip, with no flip at this step and no renewal statistic
+//    firing (every statistic already holds this well): the barrier state,
+//    pending flip and state-1 run change as in the general step's cell
+//    entry, the ring is written through, the transition-path clocks restart.
+template <bool DBL>
+__device__ __forceinline__ int light_step(const JobF* jobs, const SlotsDev& S, RareSm& sm, int t, int64_t slot,
+                                          int job, uint32_t traj, uint64_t s, bool countdown, float& xp, float& lo,
+                                          float& hi, float& F, int& lrel) {
+    const JobF& J = jobs[job];
+    const long long nflip = sm.nflip[t];
+    if (countdown) {
+        const long long nxf = sm.nxf[t];
+        if (!(xp > lo && xp < hi) || (long long)s != nxf || (long long)s == nflip || s == J.nsteps || J.write_x)
+            return 0;
+        const int fidx = sm.fidx[t];
+        if (fidx < J.nframe && J.fx) J.fx[(int64_t)fidx * J.ntraj + traj] = (double)sm.cell[t] * J.Ld + (double)xp;
+        sm.fidx[t] = fidx + 1;
+        const long long nx2 = nxf + (long long)J.freq_save;
+        sm.nxf[t] = nx2;
+        lrel = steps_to_special(J, s, nx2, nflip);
+        return 2;
+    }
+    if ((long long)s == nflip) return 0;
+    const float hL = J.halfL;
+    int sw = sm.sw[t];
+    if (xp >= -hL && xp < hL) {
+        // inside the cell: a band change unless the well or the local
+        // barrier changes, or xp sits on a breakpoint
+        float l2, h2;
+        band_of<DBL>(J, xp, &l2, &h2);
+        if (!(xp > l2 && xp < h2)) return 0;
+        if ((xp < 0.0f) != (lo < 0.0f)) return 0;
+        if (DBL && ((xp < J.xc ? 0 : W_LB) != (sw & W_LB))) return 0;
+        lo = l2;
+        hi = h2;
+        F = force_of<DBL>(J, xp, sm.state[t]);
+        return 1;
+    }
+    if (!J.edge_flat || !J.eta) return 0;
+    float xn;
+    int dc;
+    if (xp >= hL) {
+        xn = xp - J.L;
+        dc = 1;
+        if (!(xn > -hL && xn < J.edge_lo)) return 0;
+    } else if (xp < -hL) {
+        xn = xp + J.L;
+        dc = -1;
+        if (!(xn > J.edge_hi && xn < hL)) return 0;
+    } else {
+        return 0;   // not finite
+    }
+    const int cell_prev = sm.cell[t], cell = cell_prev + dc;
+    const int well = cell - (xn < 0.0f ? 1 : 0);
+    if (well != cell_prev - (lo < 0.0f ? 1 : 0)) return 0;
+    const int lb = DBL ? (xn < J.xc ? 0 : 1) : 0;
+    if (DBL && lb == (sw & W_LB)) return 0;   // the general step enters a key only when lb changes
+    const int key_prev = fkey(DBL, cell_prev, sw & W_LB), key = fkey(DBL, cell, lb);
+    if (!(sw & W_CVALID) || sm.ckey[t] != key || sm.cflip[t] <= (long long)s) return 0;
+    const uint32_t bits = sm.bits[t];
+    const int evm = J.evm;
+    if ((evm & EV_FPT) && (bits & B_FPT_UP)) return 0;
+    if ((evm & EV_FPT2) && ((bits & B_FPT2_UP) || sm.idx2[t] != well)) return 0;
+    if ((evm & EV_TPT) && !(bits & B_TPT2_UP) && sm.tpt2w[t] != well) return 0;
+    if ((evm & EV_CG) && sm.cgw[t] != well) return 0;
+    if ((evm & EV_WT) && (bits & B_WT_PASSED)) return 0;
+    // leave key_prev (its eviction, if its entry displaced another cell's,
+    // is counted now), enter the cached key
+    const int st_prev = sm.state[t];
+    if (sw & W_EVICT) red_add(&J.counts[(int64_t)LDP_C_EVICT * J.ntraj + traj], 1);
+    S.ring[(int64_t)(key_prev & (S.ring_slots - 1)) * S.nslots + slot] =
+        make_longlong2((long long)key_prev, (nflip << 1) | (long long)st_prev);
+    const int ps = (sw & W_CSTATE) ? 1 : 0;
+    const long long nb = sm.cflip[t];
+    sm.ckey[t] = key_prev;
+    sm.cflip[t] = nflip;
+    sm.nflip[t] = nb;
+    sw = (DBL ? (lb ? W_LB : 0) : (sw & W_LB)) | W_CVALID | (st_prev ? W_CSTATE : 0);
+    sm.sw[t] = sw;
+    if (ps != st_prev) {
+        if (ps) sm.since[t] = (long long)s;
+        else sm.sc1[t] += (long long)s - sm.since[t];
+        sm.state[t] = ps;
+    }
+    sm.cell[t] = cell;
+    if (evm & EV_TPT) {
+        sm.bits[t] = bits & ~(B_TPT_UP | B_TPT2_UP);
+        sm.tpt[t] = (long long)s;
+        sm.tpt2[t] = (long long)s;
+        sm.tpt2w[t] = well;
+    }
+    xp = xn;
+    if (dc > 0) { lo = -hL; hi = J.edge_lo; }
+    else { lo = J.edge_hi; hi = hL; }
+    F = 0.0f;
+    lrel = steps_to_special(J, s, sm.nxf[t], nb);
+    return 2;
+}
+
 }  // namespace
 
 #ifndef LDP_FP32_MIN_BLOCKS
@@ -771,19 +882,27 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
             // left counts from the quad's start: the countdown ends at this
             // sub-step when it equals h + 1 (one decrement per quad)
             if (__builtin_expect(!(xp > lo && xp < hi) || left == h + 1, 0)) {
-                sm.xp[t] = xp;
-                sm.rv[t] = rv;
-                sm.F[t] = F;
-                sm.left[t] = left - (h + 1);
-                sm.lo[t] = lo;
-                sm.hi[t] = hi;
-                general_step<DBL, OVER>(q.jobs, &S, &sm, t, slot, 4 * j + 1 + h);
-                xp = sm.xp[t];
-                F = sm.F[t];
-                lo = sm.lo[t];
-                hi = sm.hi[t];
-                left = sm.left[t] + (h + 1);
-                job = sm.job[t];
+                const uint64_t s = 4 * j + 1 + h;
+                int lrel = 0;
+                const int lt = light_step<DBL>(q.jobs, S, sm, t, slot, job, traj, s, left == h + 1, xp, lo, hi, F,
+                                               lrel);
+                if (lt == 2) {
+                    left = lrel + (h + 1);
+                } else if (lt == 0) {
+                    sm.xp[t] = xp;
+                    sm.rv[t] = rv;
+                    sm.F[t] = F;
+                    sm.left[t] = left - (h + 1);
+                    sm.lo[t] = lo;
+                    sm.hi[t] = hi;
+                    general_step<DBL, OVER>(q.jobs, &S, &sm, t, slot, s);
+                    xp = sm.xp[t];
+                    F = sm.F[t];
+                    lo = sm.lo[t];
+                    hi = sm.hi[t];
+                    left = sm.left[t] + (h + 1);
+                    job = sm.job[t];
+                }
             }
             if (!OVER) rv = fmaf(F, c1, rv);
         }

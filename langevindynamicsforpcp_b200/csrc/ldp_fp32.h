@@ -45,6 +45,12 @@ struct JobF {
     float invLf;         // 1 / L
     float bp[8];         // force breakpoints in [-L/2, L/2], ascending (cell edges included)
     int32_t nbp, pad1;
+    // The bands next to the cell edges, (-L/2, edge_lo) and (edge_hi, L/2),
+    // and whether the force is zero in both (no barrier flank reaches the
+    // cell edge): then a crossing of the cell edge lands in a known flat
+    // band (the hot loop's light step).
+    float edge_lo, edge_hi;
+    int32_t edge_flat, pad2;
     // FP64 constants (step 0, events, frames)
     double x0, v0, dt, Ld, invL, sig_v0, sig_r_d, a_lap, c_lap[2], p_first, p_cell0, mhalf;
     double Hs[2], Hd[2][2], iN[2][2], iP[2][2], sNd[2][2], sPd[2][2], wd, xbd[2], lo0d, hi1d, xcd;

@@ -186,6 +186,10 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
         for (int i = 0; i < nc; ++i)
             if (c[i] >= -k.fhalfL && c[i] <= k.fhalfL && (nb == 0 || c[i] != J->bp[nb - 1])) J->bp[nb++] = c[i];
         J->nbp = nb;
+        J->edge_lo = nb >= 3 ? J->bp[1] : k.fhalfL;
+        J->edge_hi = nb >= 3 ? J->bp[nb - 2] : -k.fhalfL;
+        const bool flat = k.dbl ? (k.flo0 > -k.fhalfL && k.fhi1 < k.fhalfL) : (k.fw < k.fhalfL);
+        J->edge_flat = (nb >= 3 && flat) ? 1 : 0;
     }
     J->x0 = k.x0; J->v0 = k.v0; J->dt = k.dt; J->Ld = k.L; J->invL = k.invL; J->sig_v0 = k.sig_v0;
     J->sig_r_d = k.sig_r; J->a_lap = k.a_lap; J->c_lap[0] = k.c_lap[0]; J->c_lap[1] = k.c_lap[1];
