@@ -262,9 +262,21 @@ ldp_status  ldp_ctx_get_fp32_shape(ldp_ctx *ctx, int *block, int *grid, uint64_t
 void        ldp_params_default(int model, ldp_params *p);
 ldp_status  ldp_params_from_inp(const char *path, int model, ldp_params *p,
                                 char *err, size_t errlen);
+/* base_dir: the directory relative INCLUDE paths are opened from, at every
+ * nesting level; NULL or "" opens them relative to the working directory,
+ * as the reference does (src/inputParser.cpp:311) and ldp_params_from_inp
+ * always does. */
 ldp_status  ldp_params_from_inp_text(const char *text, const char *base_dir,
                                      int model, ldp_params *p,
                                      char *err, size_t errlen);
+/* The reference's `-p` (InputParser::PrintAllValues, src/inputParser.cpp:
+ * 188-196): every option of the parsed file in option-table order, one line
+ * "%-20s %3d %s\n" per occurrence (key, occurrence index, its values joined
+ * by single spaces), written to buf as a NUL-terminated string.  *needed
+ * (if not NULL) receives the bytes required; LDP_ERR_NOMEM when buflen is
+ * smaller.  On a parse error buf holds the message. */
+ldp_status  ldp_inp_print_values(const char *path, int model, char *buf,
+                                 size_t buflen, size_t *needed);
 /* Writes the default .inp (the reference's `-o file.inp`,
  * src/inputParser.cpp:212-266). */
 ldp_status  ldp_write_default_inp(const char *path, int model);

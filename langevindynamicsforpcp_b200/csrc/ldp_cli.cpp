@@ -79,11 +79,16 @@ int main(int argc, char** argv) {
         return 1;
     }
     if (print) {
-        std::fprintf(stderr, "OUTPUTBASE %s\nOVERDAMPED %d\nX0 %.17g\nTIMESTEP %.17g\nNUMBEROFSTEPS %llu\n"
-                             "FREQSAVE %llu\nTAU %.17g\nRANDOMSEED %lld\n",
-                     p.output_base, p.overdamped, p.x0, p.timestep, (unsigned long long)p.number_of_steps,
-                     (unsigned long long)p.freq_save, p.tau, (long long)p.random_seed);
-        return 0;
+        // every parsed option, as the reference's PrintAllValues
+        size_t need = 0;
+        std::string buf(1 << 16, '\0');
+        st = ldp_inp_print_values(in, LDP_CLI_MODEL, &buf[0], buf.size(), &need);
+        if (st == LDP_ERR_NOMEM) {
+            buf.assign(need, '\0');
+            st = ldp_inp_print_values(in, LDP_CLI_MODEL, &buf[0], buf.size(), &need);
+        }
+        std::fputs(buf.c_str(), stderr);
+        return st == LDP_OK ? 0 : 1;
     }
     ldp_ctx* ctx = nullptr;
     st = ldp_create(&ctx, device);

@@ -270,8 +270,9 @@ struct Parser {
                     }
                     std::stringstream ss;
                     ss << f.rdbuf();
-                    std::string sub_base = path.find('/') == std::string::npos ? base_dir : path.substr(0, path.rfind('/'));
-                    if (!open_text(ss.str(), sub_base, depth + 1)) return false;
+                    // nested INCLUDEs resolve against the same base (the
+                    // working directory unless the caller gave one)
+                    if (!open_text(ss.str(), base_dir, depth + 1)) return false;
                 }
             } else if (iequals(w[0], "define")) {
                 if (w.size() != 3) {
@@ -317,6 +318,49 @@ void set_str(char* dst, const std::string& s) { std::snprintf(dst, LDP_PATH_MAX,
 
 extern "C" void ldp_params_default(int model, ldp_params* p);
 
+// Reads the .inp text into per-option value lists (option table order, one
+// entry per occurrence, each the occurrence's values): OpenInput and
+// ProcessInputLines, src/inputParser.cpp:269-330, 412-475.
+static ldp_status parse_values(const char* text, const char* base_dir, int model, Table* tb,
+                               std::vector<std::vector<std::vector<std::string>>>* vals, std::string* err) {
+    Parser ps;
+    if (!ps.open_text(text, base_dir ? base_dir : "", 0)) {
+        *err = ps.err;
+        return LDP_ERR_PARSE;
+    }
+    *tb = table_for(model);
+    std::map<std::string, int> idx;
+    for (int i = 0; i < tb->n; ++i) idx[tb->opts[i].key] = i;
+    vals->assign(tb->n, {});
+    for (const std::string& l : ps.content) {
+        if (is_blank(l)) continue;
+        std::vector<std::string> w = split_ws(l);
+        auto it = idx.find(w[0]);
+        if (it == idx.end()) {
+            *err = "undefined option (" + w[0] + ")";
+            return LDP_ERR_PARSE;
+        }
+        const Opt& o = tb->opts[it->second];
+        std::vector<std::string> v(w.begin() + 1, w.end());
+        if (!o.multiple && !(*vals)[it->second].empty()) {
+            *err = "(" + w[0] + ") can be specified only once";
+            return LDP_ERR_PARSE;
+        }
+        if ((int)v.size() != o.nval) {
+            *err = "(" + w[0] + ") requires exactly " + std::to_string(o.nval) + " values but got " +
+                   std::to_string(v.size()) + " (" + join(w, 1) + ")";
+            return LDP_ERR_PARSE;
+        }
+        (*vals)[it->second].push_back(v);
+    }
+    for (int i = 0; i < tb->n; ++i)
+        if ((*vals)[i].empty()) {
+            *err = std::string("(") + tb->opts[i].key + ") must be specified at least once";
+            return LDP_ERR_PARSE;
+        }
+    return LDP_OK;
+}
+
 extern "C" ldp_status ldp_params_from_inp_text(const char* text, const char* base_dir, int model, ldp_params* p,
                                                char* err, size_t errlen) {
     auto fail = [&](ldp_status st, const std::string& m) {
@@ -325,30 +369,13 @@ extern "C" ldp_status ldp_params_from_inp_text(const char* text, const char* bas
     };
     if (!text || !p) return fail(LDP_ERR_INVALID, "null argument");
     if (model != LDP_MODEL_SINGLE && model != LDP_MODEL_DOUBLE) return fail(LDP_ERR_INVALID, "unknown model");
-    Parser ps;
-    if (!ps.open_text(text, base_dir ? base_dir : "", 0)) return fail(LDP_ERR_PARSE, ps.err);
-    Table tb = table_for(model);
+    Table tb;
+    std::vector<std::vector<std::vector<std::string>>> vals;
+    std::string perr;
+    const ldp_status pst = parse_values(text, base_dir, model, &tb, &vals, &perr);
+    if (pst != LDP_OK) return fail(pst, perr);
     std::map<std::string, int> idx;
     for (int i = 0; i < tb.n; ++i) idx[tb.opts[i].key] = i;
-    std::vector<std::vector<std::vector<std::string>>> vals(tb.n);
-    // ProcessInputLines, src/inputParser.cpp:412-475.
-    for (const std::string& l : ps.content) {
-        if (is_blank(l)) continue;
-        std::vector<std::string> w = split_ws(l);
-        auto it = idx.find(w[0]);
-        if (it == idx.end()) return fail(LDP_ERR_PARSE, "undefined option (" + w[0] + ")");
-        const Opt& o = tb.opts[it->second];
-        std::vector<std::string> v(w.begin() + 1, w.end());
-        if (!o.multiple && !vals[it->second].empty())
-            return fail(LDP_ERR_PARSE, "(" + w[0] + ") can be specified only once");
-        if ((int)v.size() != o.nval)
-            return fail(LDP_ERR_PARSE, "(" + w[0] + ") requires exactly " + std::to_string(o.nval) + " values but got " +
-                                           std::to_string(v.size()) + " (" + join(w, 1) + ")");
-        vals[it->second].push_back(v);
-    }
-    for (int i = 0; i < tb.n; ++i)
-        if (vals[i].empty())
-            return fail(LDP_ERR_PARSE, std::string("(") + tb.opts[i].key + ") must be specified at least once");
 
     auto get = [&](const char* key, int j = 0, int k = 0) -> const std::string& { return vals[idx[key]][j][k]; };
     auto dbl = [&](const char* key, int k = 0) {
@@ -447,9 +474,42 @@ extern "C" ldp_status ldp_params_from_inp(const char* path, int model, ldp_param
     }
     std::stringstream ss;
     ss << f.rdbuf();
-    std::string sp(path);
-    std::string base = sp.find('/') == std::string::npos ? std::string() : sp.substr(0, sp.rfind('/'));
-    return ldp_params_from_inp_text(ss.str().c_str(), base.c_str(), model, p, err, errlen);
+    // INCLUDE paths are opened as written, i.e. relative to the working
+    // directory, as the reference's OpenInput does (src/inputParser.cpp:311).
+    return ldp_params_from_inp_text(ss.str().c_str(), "", model, p, err, errlen);
+}
+
+// PrintAllValues (src/inputParser.cpp:188-196), the reference's `-p`: every
+// option in table order, one line per occurrence, "%-20s %3d %s" with the
+// occurrence's values joined by single spaces.
+extern "C" ldp_status ldp_inp_print_values(const char* path, int model, char* buf, size_t buflen, size_t* needed) {
+    if (!path || (!buf && buflen)) return LDP_ERR_INVALID;
+    std::ifstream f(path);
+    if (!f) {
+        if (buf && buflen) std::snprintf(buf, buflen, "Error (InputParser): can't open input file (%s)\n", path);
+        return LDP_ERR_IO;
+    }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    Table tb;
+    std::vector<std::vector<std::vector<std::string>>> vals;
+    std::string perr;
+    const ldp_status st = parse_values(ss.str().c_str(), "", model, &tb, &vals, &perr);
+    if (st != LDP_OK) {
+        if (buf && buflen) std::snprintf(buf, buflen, "Error (InputParser): %s\n", perr.c_str());
+        return st;
+    }
+    std::string out;
+    char line[4096];
+    for (int i = 0; i < tb.n; ++i)
+        for (size_t j = 0; j < vals[i].size(); ++j) {
+            std::snprintf(line, sizeof(line), "%-20s %3d %s\n", tb.opts[i].key, (int)j, join(vals[i][j], 0).c_str());
+            out += line;
+        }
+    if (needed) *needed = out.size() + 1;
+    if (out.size() + 1 > buflen) return LDP_ERR_NOMEM;
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    return LDP_OK;
 }
 
 // PrintEmptyInputFile (src/inputParser.cpp:212-266): `# [Type] help` then

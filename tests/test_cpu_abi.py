@@ -69,16 +69,58 @@ def test_grammar_define_variables_continuation_for():
     assert list(p.cg_sizes[:p.n_cg]) == [2, 3, 4, 5, 10, 100, 70, 71, 72]
 
 
-def test_grammar_include(tmp_path):
+def test_grammar_include(tmp_path, monkeypatch):
+    # INCLUDE paths are opened as written, relative to the working directory
+    # (the reference's OpenInput, src/inputParser.cpp:311), not relative to
+    # the including file: main.inp in inputs/ includes parts/part.inp, which
+    # lies under the working directory.
     txt = quick_text()
     head, tail = txt[: len(txt) // 2], txt[len(txt) // 2:]
     cut = head.rfind("\n")
     head, tail = txt[:cut + 1], txt[cut + 1:]
-    (tmp_path / "part.inp").write_text(tail)
-    (tmp_path / "main.inp").write_text(head + "INCLUDE part.inp\n")
-    p = ldp.params_from_inp(str(tmp_path / "main.inp"))
+    (tmp_path / "inputs").mkdir()
+    (tmp_path / "parts").mkdir()
+    (tmp_path / "parts" / "part.inp").write_text(tail)
+    (tmp_path / "inputs" / "main.inp").write_text(head + "INCLUDE parts/part.inp\n")
+    monkeypatch.chdir(tmp_path)
+    p = ldp.params_from_inp("inputs/main.inp")
     q = ldp.params_from_inp_text(txt)
     assert bytes(p) == bytes(q)
+    # the same name next to the including file is not what the reference opens
+    monkeypatch.chdir(tmp_path / "inputs")
+    with pytest.raises(Exception, match="can't open input file"):
+        ldp.params_from_inp("main.inp")
+
+
+def test_print_values_is_the_references_print_all_values(tmp_path):
+    # `-p`: every option in option-table order, one "%-20s %3d %s" line per
+    # occurrence (InputParser::PrintAllValues, src/inputParser.cpp:188-196),
+    # on stderr; the FPTCG occurrences are numbered 0..n-1.
+    path = os.path.join(GOLDEN, "quick_test__2.0_7.2_m1.0_1.00e-05.inp")
+    entries = {}
+    for ln in open(path):
+        w = ln.split("#")[0].split()
+        if not w:
+            continue
+        if w[0] not in entries:
+            entries[w[0]] = []
+        entries[w[0]].append(" ".join(w[1:]))
+    exe = os.path.join(ROOT, "langevindynamicsforpcp_b200", "bin", "langevinDynamicsSingleBarrier")
+    import subprocess
+    r = subprocess.run([exe, "-i", path, "-p"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    lines = r.stderr.splitlines()
+    parsed = []
+    for l in lines:
+        m = re.match(r"^(\S+) +(\d+) (.*)$", l)
+        assert m, l
+        key, idx, val = m.group(1), int(m.group(2)), m.group(3)
+        assert l == "%-20s %3d %s" % (key, idx, val)
+        assert entries[key][idx] == val
+        parsed.append((key, idx))
+    assert parsed[0][0] == "OUTPUTBASE" and parsed[-1][0] == "PRINTTIMER"
+    assert len(lines) == sum(len(v) for v in entries.values())
+    assert [i for k, i in parsed if k == "FPTCG"] == list(range(7))
 
 
 @pytest.mark.parametrize("edit,msg", [
