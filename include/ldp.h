@@ -128,7 +128,13 @@ typedef struct ldp_job_opts {
     int32_t keep_frames;      /* keep x frames on the device after the MSD
                                  (needed for ldp_job_traj_results frames);
                                  default 1                                   */
-    int32_t pad;
+    int32_t first_rank;       /* the job is virtual ranks first_rank ..
+                                 first_rank + ranks - 1 of a larger run: its
+                                 trajectory i draws the random streams of
+                                 trajectory first_rank*runs*lanes + i, restart
+                                 files and trajectory dumps carry the global
+                                 rank, so ranks split over processes or GPUs
+                                 give the whole run's trajectories; default 0 */
     int64_t event_cap;        /* per-event lists kept per trajectory and list
                                  (ldp_event_list; FP64 plain, fixed steps):
                                  the reference's per-lane event vectors that

@@ -88,13 +88,15 @@ class Job:
     def __init__(self, ctx: Context, params: Params, lanes: int = 8, ranks: int = 1,
                  precision: int = PREC_FP64_PLAIN, mode: int = MODE_FIXED_STEPS,
                  step_cap: int = 100_000_000, table_slots: int = 256, tick_cap: int = -1,
-                 job_id: int = 0, steps_per_launch: int = 0, block_size: int = 0, event_cap: int = 0):
+                 job_id: int = 0, steps_per_launch: int = 0, block_size: int = 0, event_cap: int = 0,
+                 first_rank: int = 0):
         self.ctx = ctx
         o = JobOpts()
         L.lib().ldp_job_opts_default(C.byref(o))
         o.lanes, o.ranks, o.precision, o.mode = lanes, ranks, precision, mode
         o.step_cap, o.table_slots, o.tick_cap, o.job_id = step_cap, table_slots, tick_cap, job_id
         o.steps_per_launch, o.block_size, o.event_cap = steps_per_launch, block_size, event_cap
+        o.first_rank = first_rank
         self.opts = o
         self.params = params
         h = C.c_void_p()

@@ -71,7 +71,7 @@ class JobOpts(C.Structure):
         ("lanes", C.c_int32), ("ranks", C.c_int32), ("precision", C.c_int32), ("mode", C.c_int32),
         ("step_cap", C.c_uint64), ("table_slots", C.c_int32), ("tick_cap", C.c_int64),
         ("job_id", C.c_uint32), ("steps_per_launch", C.c_uint64), ("block_size", C.c_int32),
-        ("keep_frames", C.c_int32), ("pad", C.c_int32), ("event_cap", C.c_int64),
+        ("keep_frames", C.c_int32), ("first_rank", C.c_int32), ("event_cap", C.c_int64),
     ]
 
 

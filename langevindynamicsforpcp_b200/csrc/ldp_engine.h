@@ -29,6 +29,7 @@ struct KConst {
     int32_t cg_size[LDP_MAX_CG];
     int32_t write_x, fp_mode, lanes, nruns, slots, at_bottom;
     uint32_t key0, key1;
+    uint32_t g0;             // stream index of the job's trajectory 0 (first_rank * runs * lanes)
     double x0, v0, dt, L, invL;
     double w, Hs[2], slope[2];
     double xb[2], lo0, hi1, xc;

@@ -231,7 +231,7 @@ __device__ __noinline__ void f_start(const JobF* Jp, longlong2* ring, int64_t ns
                                      uint32_t traj, RareSm* sm, int t, float* xp, float* rv, int* cell, int* state,
                                      int* sw) {
     const JobF& J = *Jp;
-    const uint32_t g = traj;
+    const uint32_t g = traj + J.g0;   // the trajectory's random streams
     for (int r = 0; r < ring_slots; ++r) ring[(int64_t)r * nslots + slot] = make_longlong2((long long)INT64_MIN, 0);
     const double red = J.x0 * J.invL;
     const int c = (int)rint(red);
@@ -275,7 +275,7 @@ __device__ __noinline__ void f_start(const JobF* Jp, longlong2* ring, int64_t ns
     sm->cgw[t] = INT32_MIN;
     sm->fidx[t] = 1;
     sm->nxf[t] = (!J.fp_mode && J.freq_save) ? (long long)J.freq_save : INT64_MAX;
-    sm->nflip[t] = next_flip(J, traj, 0, st);
+    sm->nflip[t] = next_flip(J, g, 0, st);
     sm->fpt[t] = sm->fpt2[t] = sm->tpt[t] = sm->tpt2[t] = 0;
     sm->cflip[t] = 0;
     sm->sc1[t] = 0;
@@ -360,6 +360,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     if (job < 0) return;
     const JobF& J = jobs[job];
     const uint32_t traj = sm.traj[t];
+    const uint32_t gp = traj + J.g0;   // the trajectory's random streams
     float xp = sm.xp[t];
     const float rv = sm.rv[t];
     float lo = sm.lo[t], hi = sm.hi[t];
@@ -403,7 +404,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
                 ps = (int)(e.y & 1);
                 nb = e.y >> 1;
             } else {
-                ps = f_default_state(J, DBL, traj, key_cur);
+                ps = f_default_state(J, DBL, gp, key_cur);
                 nb = 0;
                 found = false;
                 ev = e.x != (long long)INT64_MIN;
@@ -422,9 +423,9 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
         // uniform the FP64 path draws.
         const int sb = found ? (ps ^ 1) : ps;
         const float pl = J.c_lapf[J.eq ? 0 : sb] * one_minus_exp(J.a_lapf * (float)((long long)s - nb));
-        const uint32_t w0 = philox_at(s, traj, TAG_CATCHUP, J.key0, J.key1).w0;
+        const uint32_t w0 = philox_at(s, gp, TAG_CATCHUP, J.key0, J.key1).w0;
         const int sn = ((pl >= 1.0f) || (w0 < (uint32_t)(pl * 4294967296.0f))) ? (sb ^ 1) : sb;
-        if (!have_wf) *wf = philox_at(s, traj, TAG_FLIP, J.key0, J.key1);
+        if (!have_wf) *wf = philox_at(s, gp, TAG_FLIP, J.key0, J.key1);
         *nf = flip_schedule(s, wf->w2, wf->w3, J.ln1m[sn]);
         return sn;
     };
@@ -456,8 +457,8 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
                     bits &= ~(B_FPT_UP | B_INIT0 | B_INIT1);
                     sm.fpt[t] = now;
                     int s0, s1, i0;
-                    if (well == cell) { s0 = state; s1 = f_ring_state(J, S, slot, false, traj, cell + 1); i0 = cell; }
-                    else { s0 = f_ring_state(J, S, slot, false, traj, cell - 1); s1 = state; i0 = cell - 1; }
+                    if (well == cell) { s0 = state; s1 = f_ring_state(J, S, slot, false, gp, cell + 1); i0 = cell; }
+                    else { s0 = f_ring_state(J, S, slot, false, gp, cell - 1); s1 = state; i0 = cell - 1; }
                     sm.init0[t] = i0;
                     bits |= (s0 ? B_INIT0 : 0u) | (s1 ? B_INIT1 : 0u);
                 }
@@ -578,7 +579,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     long long nf = sm.nflip[t];
     Words wf{};
     if (flip) {
-        wf = philox_at(s, traj, TAG_FLIP, J.key0, J.key1);
+        wf = philox_at(s, gp, TAG_FLIP, J.key0, J.key1);
         nf = flip_schedule(s, wf.w0, wf.w1, J.ln1m[st]);
     }
     if (dKey) st = enter(fkey(DBL, cell_prev, lb_prev), st, fkey(DBL, cell, lb), &nf, &wf, flip);
@@ -748,7 +749,9 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
 
     // ---- hot lane state (registers); the rest lives in sm ----
     int job = (slot < S.nslots) ? S.job[slot] : -1;
-    uint32_t traj = 0;
+    // the lane's trajectory: job-local index in sm.traj, its random-stream
+    // index (plus the job's g0) in a register
+    uint32_t ptraj = 0;
     uint64_t j = 0;                 // next block of four steps: 4j+1 .. 4j+4
     float xp = 0.f, rv = 0.f, F = 0.f, lo = -kInf, hi = kInf;
     int left = kLeftMax;
@@ -758,7 +761,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
 
     // Per-job constants into registers; band, force and countdown from the
     // position.  s = next step.
-    auto bind = [&](uint64_t s) {
+    auto bind = [&](uint32_t traj, uint64_t s) {
         const JobF& J = q.jobs[job];
         if (OVER) c1 = J.c_drift;
         else { c1 = J.hdt_invM; c2 = J.hdt; c3 = J.expg; }
@@ -767,6 +770,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         kn = J.bm_k;
         key0 = J.key0;
         key1 = J.key1;
+        ptraj = traj + J.g0;
         const int state = sm.state[t];
         band_of<DBL>(J, xp, &lo, &hi);
         F = force_of<DBL>(J, xp, state);
@@ -776,7 +780,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
 
     if (job >= 0) {
         const JobF& J = q.jobs[job];
-        traj = (uint32_t)S.traj[slot];
+        const uint32_t traj = (uint32_t)S.traj[slot];
         const uint64_t s = (uint64_t)S.step[slot];
         xp = S.xp[slot];
         rv = S.rv[slot];
@@ -800,7 +804,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         sm.fidx[t] = S.fidx[slot];
         sm.nxf[t] = S.nxf[slot];
         sm.nflip[t] = S.nflip[slot];
-        bind(s);
+        bind(traj, s);
     }
 
     bool dry = false;   // the queue had nothing left for this warp
@@ -834,13 +838,13 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
                 if (need) {
                     const unsigned rank = __popc(m & ((1u << lane) - 1u));
                     if (rank < got) {
-                        traj = (uint32_t)f_resolve(q.range_end, q.range_job, q.range_first, q.nranges,
+                        const uint32_t traj = (uint32_t)f_resolve(q.range_end, q.range_job, q.range_first, q.nranges,
                                                    (int64_t)(base + rank), &job);
                         const JobF* Jn = &q.jobs[job];
                         f_start<DBL, OVER>(Jn, S.ring, S.nslots, S.ring_slots, slot, traj, &sm, t, &xp, &rv,
                                            &sm.cell[t], &sm.state[t], &sm.sw[t]);
                         sm.job[t] = job;
-                        bind(1);
+                        bind(traj, 1);
                         if (Jn->nsteps == 0) {
                             retire_lane<OVER>(*Jn, S.retired, sm, t, 0, xp, rv, 0);
                             job = -1;
@@ -861,7 +865,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         }
 
         // ---- one Philox block, four steps ----
-        const Words w = philox_wide((uint32_t)j, (uint32_t)(j >> 32), traj, TAG_STEP, key0, key1);
+        const Words w = philox_wide((uint32_t)j, (uint32_t)(j >> 32), ptraj, TAG_STEP, key0, key1);
         float nq[4];
         noise_pair(w.w0, w.w1, kn, &nq[0], &nq[1]);
         noise_pair(w.w2, w.w3, kn, &nq[2], &nq[3]);
@@ -884,7 +888,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
             if (__builtin_expect(!(xp > lo && xp < hi) || left == h + 1, 0)) {
                 const uint64_t s = 4 * j + 1 + h;
                 int lrel = 0;
-                const int lt = light_step<DBL>(q.jobs, S, sm, t, slot, job, traj, s, left == h + 1, xp, lo, hi, F,
+                const int lt = light_step<DBL>(q.jobs, S, sm, t, slot, job, sm.traj[t], s, left == h + 1, xp, lo, hi, F,
                                                lrel);
                 if (lt == 2) {
                     left = lrel + (h + 1);
@@ -914,6 +918,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
     S.job[slot] = job;
     if (job >= 0) {
         const JobF& J = q.jobs[job];
+        const uint32_t traj = sm.traj[t];
         S.traj[slot] = traj;
         S.step[slot] = (int64_t)(4 * j + 1);
         S.xp[slot] = xp;

@@ -37,6 +37,7 @@ struct JobF {
     int32_t evm;         // EV_* statistics switches of the event path
     int32_t cg_size[LDP_MAX_CG];
     uint32_t key0, key1;
+    uint32_t g0;         // stream index of the job's trajectory 0 (first_rank * runs * lanes)
     // FP32 step constants
     float L, halfL, w, slope[2], xb[2], lo0, hi1, xc, sN[2][2], sP[2][2];
     float c_drift, sig_r, hdt_invM, hdt, expg, sig_v;

@@ -153,6 +153,7 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
     }
     for (int j = 0; j < LDP_MAX_CG; ++j) J->cg_size[j] = k.cg_size[j] ? k.cg_size[j] : 1;
     J->key0 = k.key0; J->key1 = k.key1;
+    J->g0 = k.g0;
     J->L = k.fL; J->halfL = k.fhalfL; J->w = k.fw;
     J->slope[0] = k.fslope[0]; J->slope[1] = k.fslope[1];
     J->xb[0] = k.fxb[0]; J->xb[1] = k.fxb[1]; J->lo0 = k.flo0; J->hi1 = k.fhi1; J->xc = k.fxc;

@@ -193,6 +193,7 @@ extern "C" void ldp_job_opts_default(ldp_job_opts* o) {
     o->steps_per_launch = 0;
     o->block_size = 0;
     o->keep_frames = 1;
+    o->first_rank = 0;
     o->event_cap = -1;
 }
 
@@ -225,6 +226,11 @@ static ldp_status validate(ldp_ctx* ctx, const ldp_params& p, const ldp_job_opts
     }
     if (o.lanes < 1 || o.ranks < 1 || p.number_of_runs < 1) {
         ldp_set_error(ctx, "lanes, ranks and NUMBEROFRUNS must be >= 1");
+        return LDP_ERR_INVALID;
+    }
+    if (o.first_rank < 0 ||
+        ((int64_t)o.first_rank + o.ranks) * (int64_t)p.number_of_runs * o.lanes > ((int64_t)1 << 32)) {
+        ldp_set_error(ctx, "first_rank must be >= 0 and (first_rank + ranks) x runs x lanes at most 2^32");
         return LDP_ERR_INVALID;
     }
     if (o.table_slots < 16 || (o.table_slots & (o.table_slots - 1))) {
@@ -523,7 +529,7 @@ static ldp_status submit_on(ldp_ctx* ctx, ldp_job* job, cudaStream_t s) {
         CUDA_OR_FAIL(ctx, cudaEventRecord(job->ev[0], s));
         int e = 0;
         if (!job->restored) {
-            e = launch_fp64_init(job->k, job->st, 0, job->o.block_size, s);
+            e = launch_fp64_init(job->k, job->st, job->k.g0, job->o.block_size, s);
             if (e) {
                 ldp_set_error(ctx, "init launch failed: %s", cudaGetErrorString((cudaError_t)e));
                 return LDP_ERR_DEVICE;
@@ -536,7 +542,7 @@ static ldp_status submit_on(ldp_ctx* ctx, ldp_job* job, cudaStream_t s) {
         const uint64_t first = job->steps_before + 1, last = job->steps_before + job->nsteps;
         for (uint64_t s0 = first; s0 <= last; s0 += spl) {
             const uint64_t s1 = std::min<uint64_t>(s0 + spl, last + 1);
-            e = launch_fp64_steps(job->k, job->st, 0, s0, s1, job->o.block_size, s);
+            e = launch_fp64_steps(job->k, job->st, job->k.g0, s0, s1, job->o.block_size, s);
             if (e) {
                 ldp_set_error(ctx, "step launch failed: %s", cudaGetErrorString((cudaError_t)e));
                 return LDP_ERR_DEVICE;

@@ -99,6 +99,10 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
         set_err(err, errlen, m);
         return LDP_ERR_INVALID;
     }
+    if (o->first_rank < 0 || ((int64_t)o->first_rank + o->ranks) * p->number_of_runs * o->lanes > ((int64_t)1 << 32)) {
+        set_err(err, errlen, "first_rank must be >= 0 and (first_rank + ranks) x runs x lanes at most 2^32");
+        return LDP_ERR_INVALID;
+    }
     const int slots = o->table_slots;
     if (slots < 16 || slots > LDP_NOALLOC_MAX_SLOTS || (slots & (slots - 1))) {
         char m[160];
@@ -186,7 +190,7 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
     // The init kernel writes every field of every trajectory, clears the
     // cell-table rings and zeroes the counts and sums: no state of an earlier
     // call survives into this one.
-    int e = ldp::launch_fp64_init(k, S, 0, 128, stream);
+    int e = ldp::launch_fp64_init(k, S, k.g0, 128, stream);
     if (e) {
         set_err(err, errlen, cudaGetErrorString((cudaError_t)e));
         return LDP_ERR_DEVICE;
@@ -201,7 +205,7 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
     const uint64_t nsteps = ldp::effective_steps(*p);
     for (uint64_t s0 = 1; s0 <= nsteps; s0 += spl) {
         const uint64_t s1 = std::min<uint64_t>(s0 + spl, nsteps + 1);
-        e = ldp::launch_fp64_steps(k, S, 0, s0, s1, 128, stream);
+        e = ldp::launch_fp64_steps(k, S, k.g0, s0, s1, 128, stream);
         if (e) {
             set_err(err, errlen, cudaGetErrorString((cudaError_t)e));
             return LDP_ERR_DEVICE;

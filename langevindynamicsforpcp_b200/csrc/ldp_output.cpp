@@ -464,7 +464,7 @@ static ldp_status write_outputs_timed(ldp_job* job, const char* dir, double t_to
         for (int64_t g = 0; g < n; ++g) {
             const int lane = (int)(g % W.lanes);
             const int trial = (int)((g / W.lanes) % W.nruns);
-            const int rk = (int)(g / ((int64_t)W.lanes * W.nruns));
+            const int rk = job->o.first_rank + (int)(g / ((int64_t)W.lanes * W.nruns));   // rank in the run
             char b[256];
             std::snprintf(b, sizeof(b), "%s_trajectory_%010d_%010d_%010d.log", base.c_str(), trial, lane, rk);
             FILE* f = W.open(b);

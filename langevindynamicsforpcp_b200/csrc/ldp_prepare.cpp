@@ -54,6 +54,7 @@ void prepare_kconst(const ldp_params& p, const ldp_job_opts& o, uint32_t seed, K
     k->lanes = o.lanes;
     k->nruns = p.number_of_runs;
     k->slots = o.table_slots;
+    k->g0 = (uint32_t)((int64_t)o.first_rank * p.number_of_runs * o.lanes);
     k->key0 = seed;
     k->key1 = o.job_id;
 

@@ -737,8 +737,9 @@ extern "C" ldp_status ldp_job_restore(ldp_job* job, const char* base) {
     for (int r = 0; r < ranks; ++r)
         for (int t = 0; t < runs; ++t) {
             File& f = files[(size_t)r * runs + t];
-            const std::string path = file_name(base, r, t);
-            if (!decode_path(p, path, &f, &err) || !check_header(*job, r, f, &err)) {
+            const int rg = job->o.first_rank + r;   // the rank in the run
+            const std::string path = file_name(base, rg, t);
+            if (!decode_path(p, path, &f, &err) || !check_header(*job, rg, f, &err)) {
                 if (err.find(path) == std::string::npos) err += " (" + path + ")";
                 ldp_set_error(ctx, "%s", err.c_str());
                 return LDP_ERR_RESTART;
@@ -822,7 +823,7 @@ extern "C" ldp_status ldp_job_restore(ldp_job* job, const char* base) {
             const File& f = files[(size_t)r * runs + t];
             for (int l = 0; l < lanes; ++l) {
                 const int64_t i = ((int64_t)r * runs + t) * lanes + l;
-                const uint32_t g = (uint32_t)i;
+                const uint32_t g = (uint32_t)i + k.g0;
                 const Lane& a = f.lanes[l];
                 h.x[i] = a.x; h.v[i] = a.v; h.F[i] = a.f;
                 h.rprev[i] = p.overdamped ? f.rf[l] : 0.0;
@@ -981,7 +982,7 @@ extern "C" ldp_status ldp_job_save_restart(ldp_job* job, const char* base) {
     for (int r = 0; r < ranks; ++r)
         for (int t = 0; t < runs; ++t) {
             File f;
-            fill_header(*job, r, S, &f);
+            fill_header(*job, job->o.first_rank + r, S, &f);
             f.lanes.assign(lanes, Lane());
             f.has_ext = true;
             f.ext_slots = slots;
@@ -1105,7 +1106,7 @@ extern "C" ldp_status ldp_job_save_restart(ldp_job* job, const char* base) {
                 T.step.assign(nc * lanes, 0);
                 for (int l = 0; l < lanes; ++l) {
                     const int64_t i = ((int64_t)r * runs + t) * lanes + l;
-                    const uint32_t g = (uint32_t)i;
+                    const uint32_t g = (uint32_t)i + k.g0;
                     for (size_t c = 0; c < nc; ++c) {
                         const int64_t id = lo_id[tb] + (int64_t)c;
                         const int64_t key = k.dbl ? id * 2 + tb : id;
@@ -1131,7 +1132,7 @@ extern "C" ldp_status ldp_job_save_restart(ldp_job* job, const char* base) {
             }
             std::vector<uint8_t> bytes;
             encode(f, layout_of(p), &bytes);
-            const std::string path = file_name(base, r, t);
+            const std::string path = file_name(base, job->o.first_rank + r, t);
             if (!write_file(path, bytes)) {
                 ldp_set_error(ctx, "can't open restart file (%s)", path.c_str());
                 return LDP_ERR_IO;

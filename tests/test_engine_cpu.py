@@ -1,7 +1,8 @@
 """The C++ mirror of the reference's engine interface (include/ldp_engine.hpp)
 builds against the library and keeps the reference's error convention on
 the CPU: with no device context Integrate returns false after printing the
-error, as does a trial past NUMBEROFRUNS."""
+error, as does a trial past NUMBEROFRUNS; a getter before Integrate prints
+an error and returns NaN."""
 import os
 import shutil
 import subprocess
@@ -26,5 +27,5 @@ def test_engine_mirror_reports_errors_like_the_reference(tmp_path):
     build(exe)
     r = subprocess.run([str(exe), INP, "20000", "nodevice"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.split() == ["0", "0"]
-    assert r.stderr.count("Error:") == 2
+    assert r.stdout.split() == ["0", "0", "1"]
+    assert r.stderr.count("Error:") == 3

@@ -1,7 +1,10 @@
 """The C++ mirror of the reference's engine interface (include/ldp_engine.hpp)
 returns, trial by trial and lane by lane, the results of the same run
 through the job API: Integrate(iTrial) selects trajectory
-(rank * NUMBEROFRUNS + iTrial) * lanes + lane of the run."""
+(rank * NUMBEROFRUNS + iTrial) * lanes + lane of the run.  The object
+integrates only its own rank (a job with first_rank = rank), so this also
+checks that such a job equals its slice of the whole run bit for bit; its
+per-event lists, WRITEX series and range checks are checked too."""
 import os
 import shutil
 import subprocess
@@ -33,13 +36,19 @@ def test_engine_mirror_matches_the_job_api(tmp_path):
         r = j.results(ticks=False)
         means = j.means()
     nr = p.number_of_runs
+    nf = r["frames_x"].shape[0]
     assert len(rows) == 8 * nr
-    for trial, lane, cnt, fpt, fpt2, tpt, s0, s1, xl in rows:
+    for trial, lane, cnt, fpt, fpt2, tpt, s0, s1, xl, evm, ntpt2, xnan, nv, v0 in rows:
         g = (1 * nr + int(trial)) * 8 + int(lane)
         assert int(cnt) == r["counts"][L.C_FPT][g]
         assert float(fpt) == means[L.E_FPT][g] and float(fpt2) == means[L.E_FPT2][g]
         assert float(tpt) == means[L.E_TPT][g]
         assert float(s0) == r["counts"][L.C_STATE0][g] and float(s1) == r["counts"][L.C_STATE1][g]
         assert float(xl) == r["frames_x"][-1][g]
+        # the per-event list, summed in event order, gives the average
+        assert float(evm) == (float(fpt) if int(cnt) else -1.0)
+        assert int(ntpt2) == r["counts"][L.C_TPT2][g]
+        assert xnan == "1"
+        assert int(nv) == nf and float(v0) == r["frames_v"][0][g]
     # 40 time units against a mean first-passage time of about 39: events
     assert np.sum(r["counts"][L.C_FPT]) > 0

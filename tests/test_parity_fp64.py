@@ -190,3 +190,28 @@ def test_fp64_batch_jobs_side_by_side_equal_each_alone(ctx):
             alone["lags"], alone["msd"] = job.msd()
         for k in ("counts", "sums", "x_final", "frames_x", "msd"):
             np.testing.assert_array_equal(got[i][k], alone[k], err_msg=f"job {i} {k}")
+
+
+@pytest.mark.parametrize("precision", [ldp.PREC_FP64_PLAIN, ldp.PREC_FP32_BATCHED])
+def test_rank_slice_job_equals_its_slice_of_the_run(ctx, precision):
+    # A job of ranks 2..3 of a 4-rank run (first_rank 2) draws the streams
+    # of those ranks' trajectories: it equals the whole run's slice bit for
+    # bit, on both paths (the FP64 one also against the oracle's slice).
+    p = quick(steps=60_000, freq=20, uniform_initial_states=1)
+    p.number_of_runs, p.random_seed = 2, 1234
+    lanes = 64
+    with ldp.Job(ctx, p, lanes=lanes, ranks=4, precision=precision, job_id=3) as whole:
+        whole.run()
+        rw = whole.results()
+    with ldp.Job(ctx, p, lanes=lanes, ranks=2, first_rank=2, precision=precision, job_id=3) as part:
+        part.run()
+        rp = part.results()
+    sl = slice(2 * 2 * lanes, 4 * 2 * lanes)
+    for k in ("counts", "sums", "x_final", "state0", "v0"):
+        np.testing.assert_array_equal(rp[k], rw[k][..., sl], err_msg=k)
+    np.testing.assert_array_equal(rp["frames_x"], rw["frames_x"][:, sl])
+    if precision == ldp.PREC_FP64_PLAIN:
+        ref = O.run(p, 1234, lanes=lanes, ranks=4, traj_begin=sl.start, traj_end=sl.stop, job_id=3,
+                    tick_cap=rp["ticks"].shape[1] if "ticks" in rp else 0)
+        np.testing.assert_array_equal(rp["counts"], ref["counts"])
+        np.testing.assert_array_equal(rp["x_final"], ref["x_final"])
