@@ -258,6 +258,14 @@ ldp_status  ldp_ctx_set_fp32_shape(ldp_ctx *ctx, int block, int blocks_per_sm, u
 ldp_status  ldp_ctx_mark(ldp_ctx *ctx, int mark);
 ldp_status  ldp_ctx_elapsed_ms(ldp_ctx *ctx, int mark_a, int mark_b, double *ms);
 ldp_status  ldp_ctx_synchronize(ldp_ctx *ctx);
+/* FP64 plain jobs in fixed-step mode with at most max_traj trajectories run
+ * in latency mode: one CTA of two warps per trajectory, one warp drawing
+ * the Gaussians and flip schedules of the next 32 steps while the other
+ * integrates, for runs of few long trajectories (the reference's sample:
+ * 16-32 trajectories x 3e9 steps), whose per-step dependency chain bounds
+ * them.  Results are the same bit for bit either way.  0 disables it;
+ * default 2048.  No reference counterpart. */
+ldp_status  ldp_ctx_set_fp64_latency(ldp_ctx *ctx, int64_t max_traj);
 /* The shape in effect: the resolved values once the first FP32 job ran. */
 ldp_status  ldp_ctx_get_fp32_shape(ldp_ctx *ctx, int *block, int *grid, uint64_t *pair_budget,
                                    int *ring_slots);

@@ -66,6 +66,13 @@ class Context:
     def last_error(self) -> str:
         return (L.lib().ldp_last_error(self.handle) or b"").decode()
 
+    def set_fp64_latency(self, max_traj: int) -> None:
+        """FP64 plain fixed-step jobs with at most max_traj trajectories run
+        in latency mode (ldp_ctx_set_fp64_latency; 0 disables it)."""
+        st = L.lib().ldp_ctx_set_fp64_latency(self.handle, max_traj)
+        if st != 0:
+            raise LdpError(st, "ldp_ctx_set_fp64_latency")
+
     def close(self):
         if self.handle:
             L.lib().ldp_destroy(self.handle)

@@ -76,5 +76,9 @@ int64_t frame_count(const ldp_params& p);
 int launch_fp64_init(const KConst& k, const TrajState& st, int64_t g0, int block, void* stream);
 int launch_fp64_steps(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end,
                       int block, void* stream);
+// Latency mode (few long trajectories): one CTA of a producer and a consumer
+// warp per trajectory, the same results bit for bit.
+int launch_fp64_latency(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end,
+                        void* stream);
 
 }  // namespace ldp

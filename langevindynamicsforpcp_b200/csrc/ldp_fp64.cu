@@ -261,9 +261,212 @@ __global__ void __launch_bounds__(128) fp64_init_kernel(const KConst k, const Tr
     store_traj(st, t, i);
 }
 
-// Steps s_begin .. s_end-1 of the hot loop (Integrate, S.h:1403-1511):
+// Where a step's flip schedule comes from.  FlipDraw draws it on the spot
+// (the TAG_FLIP words at the flip step, geometric waiting time in FP64) and
+// hands the words on, so that a cell entry at the same step reuses them.
+struct FlipDraw {
+    __device__ __forceinline__ int64_t schedule(const KConst& k, uint32_t g, uint64_t s, int state, Words* wf,
+                                                bool* have) const {
+        *wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+        *have = true;
+        return flip_schedule(s, wf->w0, wf->w1, k.ln1m[state]);
+    }
+};
+
+// One step s of a trajectory (Integrate's loop body, S.h:1403-1511):
 // IntegrateStepEta / IntegrateStep (S.h:1654-1706, 2833-2886; D.h:1973-2024,
 // 3448-3505) followed by UpdateStatistics (S.h:2334-2592, D.h:2931-3209).
+// z is the step's Gaussian; src supplies the flip schedule of a flip at s.
+// Returns 0 to continue, 1 when the trajectory stops before completing s
+// (non-finite position), 2 when it stops after s (first passage reached).
+template <bool DBL, bool OVER, bool ETA, class Src>
+__device__ __forceinline__ int fp64_step(const KConst& k, const TrajState& st, int64_t i, uint32_t g, T64& t,
+                                         uint64_t s, double z, const Src& src, int64_t& nflip, int64_t& sc0,
+                                         int64_t& sc1, uint32_t& flags, uint64_t& nxf) {
+    const int64_t n = st.n;
+    const uint64_t fs = k.freq_save;
+    const int64_t cell_prev = t.cell, well_prev = t.well;
+    const int lb_prev = t.lb;
+    if (OVER) {
+        const double rf = k.sig_r * z;
+        t.x = fma(t.F, k.c_drift, t.x);
+        t.x = t.x + rf;
+        t.x = t.x + t.rprev;
+        t.rprev = rf;
+    } else {
+        t.v = t.v + (k.invM * t.F) * k.hdt;
+        t.x = t.x + t.v * k.hdt;
+        t.v = k.expg * t.v + k.sig_v * z;
+        t.x = t.x + t.v * k.hdt;
+    }
+    if (!isfinite(t.x)) {
+        flags |= LDP_FLAG_NONFINITE;
+        t.bits |= B_DONE;
+        return 1;
+    }
+    indices<DBL>(k, t);
+    const bool dWell = t.well != well_prev;
+    const bool dCell = t.cell != cell_prev;
+    const bool dKey = DBL ? (t.lb != lb_prev) : dCell;
+
+    if (ETA) {
+        // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736, with
+        // every barrier's flips on a schedule (geometric waiting times of
+        // the per-step Bernoulli flips): the current barrier flips at its
+        // pending flip step; a barrier left keeps its pending flip in the
+        // cell table; one re-entered before that step has not flipped
+        // meanwhile (no draw); one whose flip came while it was away (or
+        // never visited: created at step 0) is caught up from that step
+        // with the two-state transition probability (S.h:2025-2068).
+        const bool flip = (int64_t)s == nflip;
+        Words wf{};
+        bool have_wf = false;
+        if (flip) {
+            t.state ^= 1;
+            nflip = src.schedule(k, g, s, t.state, &wf, &have_wf);
+        }
+        if (dKey) {
+            ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, nflip);
+            int ps;
+            int64_t nb;
+            bool found;
+            ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &nb, &found);
+            if (found && nb > (int64_t)s) {
+                t.state = ps;
+                nflip = nb;
+            } else {
+                const int64_t base = found ? nb : 0;
+                const int sb = found ? (ps ^ 1) : ps;
+                const double lap = (double)((int64_t)s - base);
+                const double pl = k.c_lap[k.eq ? 0 : sb] * -expm1_f64(k.a_lap * lap);
+                const uint64_t Tl = prob_to_u64(pl);
+                const Words wc = philox_at(s, g, TAG_CATCHUP, k.key0, k.key1);
+                const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
+                t.state = (U < Tl) ? (sb ^ 1) : sb;
+                if (!have_wf) wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+                nflip = flip_schedule(s, wf.w2, wf.w3, k.ln1m[t.state]);
+            }
+        }
+    } else {
+        // UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434.
+        if (dKey) {
+            ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, nflip);
+            int ps;
+            int64_t nb;
+            bool found;
+            ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &nb, &found);
+            t.state = ps;
+        }
+    }
+    if (t.state) ++sc1; else ++sc0;   // UpdateBarrierStateEtaParamter
+    energy_force<DBL>(k, t);
+    if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+
+    // UpdateStatistics.
+    if (dWell || dCell) {
+        const double now = k.dt * (double)s;
+        if (!DBL && k.wt && !k.fp_mode) {
+            if (dWell) { t.wt_tick = (int64_t)s; t.bits |= B_WT_PASSED; }
+            else if (dCell && (t.bits & B_WT_PASSED)) {
+                int64_t& nwt = st.counts[(int64_t)LDP_C_WT * n + i];
+                if (nwt < k.tick_cap) st.ticks[i * k.tick_cap + nwt] = t.wt_tick;
+                else flags |= LDP_FLAG_TICK_OVERFLOW;
+                nwt += 1;
+                t.bits &= ~B_WT_PASSED;
+            }
+        }
+        if (k.fpt || k.fp_mode) {
+            if (!DBL && !k.fp_mode) {
+                if ((t.bits & B_FPT_UP) && dCell) {
+                    t.bits &= ~B_FPT_UP;
+                    t.fpt_last = now;
+                    fpt_set_initial<DBL>(k, st, i, g, t);
+                }
+                if (!(t.bits & B_FPT_UP) && dWell) {
+                    t.bits |= B_FPT_UP;
+                    const int64_t c = st.counts[(int64_t)LDP_C_FPT * n + i];
+                    if (c == 0) st.sums[(int64_t)LDP_S_FIRST_FPT * n + i] = now - t.fpt_last;
+                    st.sums[(int64_t)LDP_S_FPT * n + i] += now - t.fpt_last;
+                    st.counts[(int64_t)LDP_C_FPT * n + i] = c + 1;
+                    const bool ib = ((double)t.cell == (double)t.init_idx0) ? ((t.bits & B_INIT0) != 0)
+                                                                            : ((t.bits & B_INIT1) != 0);
+                    if (k.ev_cap) {
+                        ev_push(k, st, LDP_E_FPT, i, c, now - t.fpt_last, &flags);
+                        if (c < k.ev_cap) st.ev_st[i * k.ev_cap + c] = (uint8_t)((t.state ? 1 : 0) | (ib ? 2 : 0));
+                    }
+                    st.counts[(int64_t)(ib ? LDP_C_INIT1 : LDP_C_INIT0) * n + i] += 1;
+                    st.counts[(int64_t)(t.state ? LDP_C_INST1 : LDP_C_INST0) * n + i] += 1;
+                }
+            }
+            if ((t.bits & B_FPT2_UP) && dCell) {
+                t.bits &= ~B_FPT2_UP;
+                t.fpt2_last = now;
+                fpt2_set_idx(t);
+            }
+            if (dCell && !(t.bits & B_FPT2_UP) && t.idx2_0 != t.cell && t.idx2_1 != t.cell) {
+                const int64_t c = st.counts[(int64_t)LDP_C_FPT2 * n + i];
+                if (c == 0) st.sums[(int64_t)LDP_S_FIRST_FPT2 * n + i] = now - t.fpt2_last;
+                st.sums[(int64_t)LDP_S_FPT2 * n + i] += now - t.fpt2_last;
+                st.counts[(int64_t)LDP_C_FPT2 * n + i] = c + 1;
+                if (k.ev_cap) ev_push(k, st, LDP_E_FPT2, i, c, now - t.fpt2_last, &flags);
+                t.fpt2_last = now;
+                fpt2_set_idx(t);
+                if (k.fp_mode) t.bits |= B_DONE;   // first passage reached
+            }
+        }
+        if (!DBL && k.tpt && !k.fp_mode) {
+            if (dCell) { t.bits &= ~B_TPT_UP; t.tpt_last = now; }
+            if (!(t.bits & B_TPT_UP) && dWell) {
+                t.bits |= B_TPT_UP;
+                const int64_t c = st.counts[(int64_t)LDP_C_TPT * n + i];
+                if (c == 0) st.sums[(int64_t)LDP_S_FIRST_TPT * n + i] = now - t.tpt_last;
+                st.sums[(int64_t)LDP_S_TPT * n + i] += now - t.tpt_last;
+                st.counts[(int64_t)LDP_C_TPT * n + i] = c + 1;
+                if (k.ev_cap) ev_push(k, st, LDP_E_TPT, i, c, now - t.tpt_last, &flags);
+            }
+            if (dCell) {
+                if (t.bits & B_TPT2_UP) t.bits &= ~B_TPT2_UP;
+                else if (t.well != t.tpt2_well) {
+                    const int64_t c = st.counts[(int64_t)LDP_C_TPT2 * n + i];
+                    if (c == 0) st.sums[(int64_t)LDP_S_FIRST_TPT2 * n + i] = now - t.tpt2_last;
+                    st.sums[(int64_t)LDP_S_TPT2 * n + i] += now - t.tpt2_last;
+                    st.counts[(int64_t)LDP_C_TPT2 * n + i] = c + 1;
+                    if (k.ev_cap) ev_push(k, st, LDP_E_TPT2, i, c, now - t.tpt2_last, &flags);
+                }
+                t.tpt2_last = now;
+                t.tpt2_well = t.well;
+            }
+        }
+        if (k.cg && !k.fp_mode && dCell) {
+            for (int jj = 0; jj < k.n_cg; ++jj) {
+                if (cg_hit(t.well, k.cg_size[jj])) {
+                    const int64_t o = (int64_t)jj * n + i;
+                    if (t.bits & (B_CG0 << jj)) {
+                        t.bits &= ~(B_CG0 << jj);
+                        st.cg_last[o] = now;
+                        st.cg_well[o] = t.well;
+                    } else if (t.well != st.cg_well[o]) {
+                        st.sums[(int64_t)(LDP_S_CG0 + jj) * n + i] += now - st.cg_last[o];
+                        const int64_t c = st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i];
+                        st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i] = c + 1;
+                        if (k.ev_cap) ev_push(k, st, LDP_E_CG0 + jj, i, c, now - st.cg_last[o], &flags);
+                        st.cg_last[o] = now;
+                        st.cg_well[o] = t.well;
+                    }
+                }
+            }
+        }
+    }
+    if (!k.fp_mode && s == nxf) {
+        record(k, st, t, i, (int64_t)(s / fs));
+        nxf += fs;
+    }
+    if (t.bits & B_DONE) return 2;
+    return 0;
+}
+
+// Steps s_begin .. s_end-1 of the hot loop, one trajectory per thread, each
+// drawing its own Gaussians (one Philox block per four steps) and flips.
 template <bool DBL, bool OVER, bool ETA>
 __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, const TrajState st, int64_t g0,
                                                          uint64_t s_begin, uint64_t s_end) {
@@ -288,6 +491,7 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
     // Gaussian pair, words 2,3 (kept) the second.
     double za = 0, zb = 0;
     uint32_t wc2 = 0, wc3 = 0;
+    const FlipDraw src;
     for (; s < s_end; ++s) {
         const int q = (int)((s - 1) & 3);
         if (q == 0 || s == s_begin) {
@@ -300,188 +504,150 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
             gauss_pair_f64(wc2, wc3, &za, &zb);
         }
         const double z = (q & 1) ? zb : za;
-
-        const int64_t cell_prev = t.cell, well_prev = t.well;
-        const int lb_prev = t.lb;
-        if (OVER) {
-            const double rf = k.sig_r * z;
-            t.x = fma(t.F, k.c_drift, t.x);
-            t.x = t.x + rf;
-            t.x = t.x + t.rprev;
-            t.rprev = rf;
-        } else {
-            t.v = t.v + (k.invM * t.F) * k.hdt;
-            t.x = t.x + t.v * k.hdt;
-            t.v = k.expg * t.v + k.sig_v * z;
-            t.x = t.x + t.v * k.hdt;
-        }
-        if (!isfinite(t.x)) {
-            flags |= LDP_FLAG_NONFINITE;
-            t.bits |= B_DONE;
-            break;
-        }
-        indices<DBL>(k, t);
-        const bool dWell = t.well != well_prev;
-        const bool dCell = t.cell != cell_prev;
-        const bool dKey = DBL ? (t.lb != lb_prev) : dCell;
-
-        if (ETA) {
-            // UpdateBarrierStateEta, S.h:1998-2153 / D.h:2435-2736, with
-            // every barrier's flips on a schedule (geometric waiting times of
-            // the per-step Bernoulli flips): the current barrier flips at its
-            // pending flip step; a barrier left keeps its pending flip in the
-            // cell table; one re-entered before that step has not flipped
-            // meanwhile (no draw); one whose flip came while it was away (or
-            // never visited: created at step 0) is caught up from that step
-            // with the two-state transition probability (S.h:2025-2068).
-            const bool flip = (int64_t)s == nflip;
-            Words wf{};
-            bool have_wf = false;
-            if (flip) {
-                t.state ^= 1;
-                wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
-                have_wf = true;
-                nflip = flip_schedule(s, wf.w0, wf.w1, k.ln1m[t.state]);
-            }
-            if (dKey) {
-                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, nflip);
-                int ps;
-                int64_t nb;
-                bool found;
-                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &nb, &found);
-                if (found && nb > (int64_t)s) {
-                    t.state = ps;
-                    nflip = nb;
-                } else {
-                    const int64_t base = found ? nb : 0;
-                    const int sb = found ? (ps ^ 1) : ps;
-                    const double lap = (double)((int64_t)s - base);
-                    const double pl = k.c_lap[k.eq ? 0 : sb] * -expm1_f64(k.a_lap * lap);
-                    const uint64_t Tl = prob_to_u64(pl);
-                    const Words wc = philox_at(s, g, TAG_CATCHUP, k.key0, k.key1);
-                    const uint64_t U = ((uint64_t)wc.w0 << 32) | wc.w1;
-                    t.state = (U < Tl) ? (sb ^ 1) : sb;
-                    if (!have_wf) wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
-                    nflip = flip_schedule(s, wf.w2, wf.w3, k.ln1m[t.state]);
-                }
-            }
-        } else {
-            // UpdateBarrierState (TAU == 0), S.h:1933-1997 / D.h:2299-2434.
-            if (dKey) {
-                ring_store(k, st, i, cell_key<DBL>(cell_prev, lb_prev), t.state, nflip);
-                int ps;
-                int64_t nb;
-                bool found;
-                ring_load<DBL>(k, st, i, g, cell_key<DBL>(t.cell, t.lb), &ps, &nb, &found);
-                t.state = ps;
-            }
-        }
-        if (t.state) ++sc1; else ++sc0;   // UpdateBarrierStateEtaParamter
-        energy_force<DBL>(k, t);
-        if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
-
-        // UpdateStatistics.
-        if (dWell || dCell) {
-            const double now = k.dt * (double)s;
-            if (!DBL && k.wt && !k.fp_mode) {
-                if (dWell) { t.wt_tick = (int64_t)s; t.bits |= B_WT_PASSED; }
-                else if (dCell && (t.bits & B_WT_PASSED)) {
-                    int64_t& nwt = st.counts[(int64_t)LDP_C_WT * n + i];
-                    if (nwt < k.tick_cap) st.ticks[i * k.tick_cap + nwt] = t.wt_tick;
-                    else flags |= LDP_FLAG_TICK_OVERFLOW;
-                    nwt += 1;
-                    t.bits &= ~B_WT_PASSED;
-                }
-            }
-            if (k.fpt || k.fp_mode) {
-                if (!DBL && !k.fp_mode) {
-                    if ((t.bits & B_FPT_UP) && dCell) {
-                        t.bits &= ~B_FPT_UP;
-                        t.fpt_last = now;
-                        fpt_set_initial<DBL>(k, st, i, g, t);
-                    }
-                    if (!(t.bits & B_FPT_UP) && dWell) {
-                        t.bits |= B_FPT_UP;
-                        const int64_t c = st.counts[(int64_t)LDP_C_FPT * n + i];
-                        if (c == 0) st.sums[(int64_t)LDP_S_FIRST_FPT * n + i] = now - t.fpt_last;
-                        st.sums[(int64_t)LDP_S_FPT * n + i] += now - t.fpt_last;
-                        st.counts[(int64_t)LDP_C_FPT * n + i] = c + 1;
-                        const bool ib = ((double)t.cell == (double)t.init_idx0) ? ((t.bits & B_INIT0) != 0)
-                                                                                : ((t.bits & B_INIT1) != 0);
-                        if (k.ev_cap) {
-                            ev_push(k, st, LDP_E_FPT, i, c, now - t.fpt_last, &flags);
-                            if (c < k.ev_cap) st.ev_st[i * k.ev_cap + c] = (uint8_t)((t.state ? 1 : 0) | (ib ? 2 : 0));
-                        }
-                        st.counts[(int64_t)(ib ? LDP_C_INIT1 : LDP_C_INIT0) * n + i] += 1;
-                        st.counts[(int64_t)(t.state ? LDP_C_INST1 : LDP_C_INST0) * n + i] += 1;
-                    }
-                }
-                if ((t.bits & B_FPT2_UP) && dCell) {
-                    t.bits &= ~B_FPT2_UP;
-                    t.fpt2_last = now;
-                    fpt2_set_idx(t);
-                }
-                if (dCell && !(t.bits & B_FPT2_UP) && t.idx2_0 != t.cell && t.idx2_1 != t.cell) {
-                    const int64_t c = st.counts[(int64_t)LDP_C_FPT2 * n + i];
-                    if (c == 0) st.sums[(int64_t)LDP_S_FIRST_FPT2 * n + i] = now - t.fpt2_last;
-                    st.sums[(int64_t)LDP_S_FPT2 * n + i] += now - t.fpt2_last;
-                    st.counts[(int64_t)LDP_C_FPT2 * n + i] = c + 1;
-                    if (k.ev_cap) ev_push(k, st, LDP_E_FPT2, i, c, now - t.fpt2_last, &flags);
-                    t.fpt2_last = now;
-                    fpt2_set_idx(t);
-                    if (k.fp_mode) t.bits |= B_DONE;   // first passage reached
-                }
-            }
-            if (!DBL && k.tpt && !k.fp_mode) {
-                if (dCell) { t.bits &= ~B_TPT_UP; t.tpt_last = now; }
-                if (!(t.bits & B_TPT_UP) && dWell) {
-                    t.bits |= B_TPT_UP;
-                    const int64_t c = st.counts[(int64_t)LDP_C_TPT * n + i];
-                    if (c == 0) st.sums[(int64_t)LDP_S_FIRST_TPT * n + i] = now - t.tpt_last;
-                    st.sums[(int64_t)LDP_S_TPT * n + i] += now - t.tpt_last;
-                    st.counts[(int64_t)LDP_C_TPT * n + i] = c + 1;
-                    if (k.ev_cap) ev_push(k, st, LDP_E_TPT, i, c, now - t.tpt_last, &flags);
-                }
-                if (dCell) {
-                    if (t.bits & B_TPT2_UP) t.bits &= ~B_TPT2_UP;
-                    else if (t.well != t.tpt2_well) {
-                        const int64_t c = st.counts[(int64_t)LDP_C_TPT2 * n + i];
-                        if (c == 0) st.sums[(int64_t)LDP_S_FIRST_TPT2 * n + i] = now - t.tpt2_last;
-                        st.sums[(int64_t)LDP_S_TPT2 * n + i] += now - t.tpt2_last;
-                        st.counts[(int64_t)LDP_C_TPT2 * n + i] = c + 1;
-                        if (k.ev_cap) ev_push(k, st, LDP_E_TPT2, i, c, now - t.tpt2_last, &flags);
-                    }
-                    t.tpt2_last = now;
-                    t.tpt2_well = t.well;
-                }
-            }
-            if (k.cg && !k.fp_mode && dCell) {
-                for (int jj = 0; jj < k.n_cg; ++jj) {
-                    if (cg_hit(t.well, k.cg_size[jj])) {
-                        const int64_t o = (int64_t)jj * n + i;
-                        if (t.bits & (B_CG0 << jj)) {
-                            t.bits &= ~(B_CG0 << jj);
-                            st.cg_last[o] = now;
-                            st.cg_well[o] = t.well;
-                        } else if (t.well != st.cg_well[o]) {
-                            st.sums[(int64_t)(LDP_S_CG0 + jj) * n + i] += now - st.cg_last[o];
-                            const int64_t c = st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i];
-                            st.counts[(int64_t)(LDP_C_CG0 + jj) * n + i] = c + 1;
-                            if (k.ev_cap) ev_push(k, st, LDP_E_CG0 + jj, i, c, now - st.cg_last[o], &flags);
-                            st.cg_last[o] = now;
-                            st.cg_well[o] = t.well;
-                        }
-                    }
-                }
-            }
-        }
-        if (!k.fp_mode && s == nxf) {
-            record(k, st, t, i, (int64_t)(s / fs));
-            nxf += fs;
-        }
-        if (t.bits & B_DONE) { ++s; break; }
+        const int r = fp64_step<DBL, OVER, ETA>(k, st, i, g, t, s, z, src, nflip, sc0, sc1, flags, nxf);
+        if (r == 1) break;
+        if (r == 2) { ++s; break; }
     }
     // s is the first step not integrated.
+    st.counts[(int64_t)LDP_C_STATE0 * n + i] = sc0;
+    st.counts[(int64_t)LDP_C_STATE1 * n + i] = sc1;
+    st.counts[(int64_t)LDP_C_STEPS * n + i] = (int64_t)s - 1;
+    if (k.fp_mode && !(t.bits & B_DONE) && s_end > k.step_cap) flags |= LDP_FLAG_CENSORED;
+    if (flags) st.counts[(int64_t)LDP_C_FLAGS * n + i] |= (int64_t)flags;
+    st.nflip[i] = nflip;
+    store_traj(st, t, i);
+}
+
+// ---------------------------------------------------------------------------
+// Latency mode: few long trajectories (the reference's own sample runs 16-32
+// trajectories for 3e9 steps).  One trajectory per thread leaves a step's
+// whole dependency chain -- Philox rounds, the FP64 logarithm and sincos of
+// Box-Muller, the flip's logarithm and division -- on one thread, ~1800
+// cycles per step.  Here a trajectory gets a CTA of two warps:
+//  * the producer warp computes, for a block of 32 steps, lane l the inputs
+//    of step s0 + l that do not depend on the position: its Gaussian (the
+//    same Philox block and Box-Muller pair the thread-per-trajectory kernel
+//    uses) and, when barriers flip, the flip schedule a flip at that step
+//    would give for either new state (its TAG_FLIP words, one logarithm,
+//    the two geometric waiting times);
+//  * lane 0 of the consumer warp runs the steps with fp64_step, taking those
+//    inputs from shared memory, so its chain is the position update,
+//    indices, flip selection and force.
+// Two buffers of 32 steps alternate; named barriers 1-2 ("full") and 3-4
+// ("empty") hand them over, every arrival matched by one wait (the producer
+// waits for the last two buffers' release before it exits).  Every input is
+// the same FP64 value, so results equal the thread-per-trajectory kernel's
+// (and the oracle's) bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kLatBlock = 32;   // steps per buffer
+
+struct LatBuf {
+    double z[2][kLatBlock];
+    int64_t cand[2][2][kLatBlock];   // [buffer][new state][step]
+};
+
+// The flip schedule of a flip at step s for both new states, from the words
+// (hi, lo) of TAG_FLIP at s: flip_schedule of either state, with the
+// logarithm evaluated once.
+__device__ __forceinline__ void flip_schedule_both(uint64_t s, uint32_t hi, uint32_t lo, const double ln1m[2],
+                                                   int64_t* c0, int64_t* c1) {
+    const double u = ((double)(((uint64_t)hi << 32) | lo) + 1.0) * 0x1p-64;
+    const double lu = log_f64(u);
+    int64_t c[2];
+#pragma unroll
+    for (int st = 0; st < 2; ++st) {
+        uint64_t wt = 0xffffffffffffffffull;
+        if (ln1m[st] < 0.0) {
+            const double q = lu / ln1m[st];
+            if (q < 0x1p62) wt = 1ull + (uint64_t)floor(q);
+        }
+        c[st] = (wt >= (uint64_t)kNeverFlip - s) ? kNeverFlip : (int64_t)(s + wt);
+    }
+    *c0 = c[0];
+    *c1 = c[1];
+}
+
+// The consumer's flip schedule source: the producer's candidates for step s.
+struct FlipFromBuffer {
+    const int64_t* c0;
+    const int64_t* c1;
+    __device__ __forceinline__ int64_t schedule(const KConst&, uint32_t, uint64_t, int state, Words*, bool*) const {
+        return state ? *c1 : *c0;
+    }
+};
+
+__device__ __forceinline__ void named_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void named_arrive(int id) { asm volatile("bar.arrive %0, 64;" ::"r"(id) : "memory"); }
+
+template <bool DBL, bool OVER, bool ETA>
+__global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, const TrajState st, int64_t g0,
+                                                          uint64_t s_begin, uint64_t s_end) {
+    __shared__ LatBuf buf;
+    const int64_t i = blockIdx.x;
+    if (i >= st.n) return;   // whole CTA: no barrier is reached
+    const uint32_t g = (uint32_t)(g0 + i);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t nblk = (s_end > s_begin) ? (s_end - s_begin + kLatBlock - 1) / kLatBlock : 0;
+    if (warp == 1) {
+        // ---- producer ----
+        for (uint64_t b = 0; b < nblk; ++b) {
+            const int u = (int)(b & 1);
+            if (b >= 2) named_sync(3 + u);   // buffer u released by the consumer
+            const uint64_t s = s_begin + b * kLatBlock + (uint64_t)lane;
+            if (s < s_end) {
+                const int q = (int)((s - 1) & 3);
+                const Words w = philox_at((s - 1) >> 2, g, TAG_STEP, k.key0, k.key1);
+                double za, zb;
+                if (q < 2) gauss_pair_f64(w.w0, w.w1, &za, &zb);
+                else gauss_pair_f64(w.w2, w.w3, &za, &zb);
+                buf.z[u][lane] = (q & 1) ? zb : za;
+                if (ETA) {
+                    const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+                    flip_schedule_both(s, wf.w0, wf.w1, k.ln1m, &buf.cand[u][0][lane], &buf.cand[u][1][lane]);
+                }
+            }
+            __syncwarp();
+            named_arrive(1 + u);             // buffer u full
+        }
+        // the consumer's release of the last two buffers
+        for (uint64_t b = (nblk > 2 ? nblk - 2 : 0); b < nblk; ++b) named_sync(3 + (int)(b & 1));
+        return;
+    }
+    // ---- consumer ----
+    T64 t;
+    int64_t sc0 = 0, sc1 = 0, nflip = 0;
+    uint32_t flags = 0;
+    uint64_t s = s_begin, nxf = 0;
+    bool run = false, active = false;
+    if (lane == 0) {
+        load_traj(st, t, i);
+        active = run = !(t.bits & B_DONE);
+        sc0 = st.counts[(int64_t)LDP_C_STATE0 * st.n + i];
+        sc1 = st.counts[(int64_t)LDP_C_STATE1 * st.n + i];
+        energy_force<DBL>(k, t);
+        nflip = st.nflip[i];
+        const uint64_t fs = k.freq_save;
+        nxf = (s_begin + fs - 1) / fs * fs;
+    }
+    for (uint64_t b = 0; b < nblk; ++b) {
+        const int u = (int)(b & 1);
+        named_sync(1 + u);                   // buffer u full
+        if (lane == 0 && run) {
+            const uint64_t s1 = (s_begin + (b + 1) * kLatBlock < s_end) ? s_begin + (b + 1) * kLatBlock : s_end;
+            for (int l = 0; s < s1; ++s, ++l) {
+                const FlipFromBuffer src{&buf.cand[u][0][l], &buf.cand[u][1][l]};
+                const int r = fp64_step<DBL, OVER, ETA>(k, st, i, g, t, s, buf.z[u][l], src, nflip, sc0, sc1, flags,
+                                                        nxf);
+                if (r == 1) { run = false; break; }
+                if (r == 2) { ++s; run = false; break; }
+            }
+        }
+        __syncwarp();
+        named_arrive(3 + u);                 // buffer u released
+    }
+    if (lane != 0 || !active) return;   // a trajectory done before the launch keeps its state
+    // s is the first step not integrated
+    const int64_t n = st.n;
     st.counts[(int64_t)LDP_C_STATE0 * n + i] = sc0;
     st.counts[(int64_t)LDP_C_STATE1 * n + i] = sc1;
     st.counts[(int64_t)LDP_C_STEPS * n + i] = (int64_t)s - 1;
@@ -511,6 +677,30 @@ static int launch_steps_t(const KConst& k, const TrajState& st, int64_t g0, uint
     const int64_t grid = (st.n + block - 1) / block;
     fp64_steps_kernel<DBL, OVER, ETA><<<(unsigned)grid, block, 0, stream>>>(k, st, g0, s0, s1);
     return (int)cudaGetLastError();
+}
+
+template <bool DBL, bool OVER, bool ETA>
+static int launch_latency_t(const KConst& k, const TrajState& st, int64_t g0, uint64_t s0, uint64_t s1,
+                            cudaStream_t stream) {
+    fp64_latency_kernel<DBL, OVER, ETA><<<(unsigned)st.n, 64, 0, stream>>>(k, st, g0, s0, s1);
+    return (int)cudaGetLastError();
+}
+
+int launch_fp64_latency(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end,
+                        void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (st.n <= 0) return 0;
+    const int sel = (k.dbl ? 4 : 0) | (k.over ? 2 : 0) | (k.eta ? 1 : 0);
+    switch (sel) {
+        case 0: return launch_latency_t<false, false, false>(k, st, g0, s_begin, s_end, s);
+        case 1: return launch_latency_t<false, false, true>(k, st, g0, s_begin, s_end, s);
+        case 2: return launch_latency_t<false, true, false>(k, st, g0, s_begin, s_end, s);
+        case 3: return launch_latency_t<false, true, true>(k, st, g0, s_begin, s_end, s);
+        case 4: return launch_latency_t<true, false, false>(k, st, g0, s_begin, s_end, s);
+        case 5: return launch_latency_t<true, false, true>(k, st, g0, s_begin, s_end, s);
+        case 6: return launch_latency_t<true, true, false>(k, st, g0, s_begin, s_end, s);
+        default: return launch_latency_t<true, true, true>(k, st, g0, s_begin, s_end, s);
+    }
 }
 
 int launch_fp64_steps(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end, int block,

@@ -15,6 +15,9 @@ struct Fp32Runtime;
 
 constexpr int kCtxMarks = 16;
 constexpr int kCtxF64Streams = 2;   // streams FP64 plain jobs of a batch share
+// FP64 plain fixed-step jobs of at most this many trajectories run in
+// latency mode (a CTA per trajectory) by default.
+constexpr int64_t kFp64LatencyMaxTraj = 2048;
 
 struct ldp_ctx {
     cudaEvent_t marks[kCtxMarks] = {};   // ldp_ctx_mark / ldp_ctx_elapsed_ms
@@ -29,6 +32,7 @@ struct ldp_ctx {
     int fp32_blocks_per_sm = 0;    // resident blocks per SM (0: default 4)
     uint64_t fp32_pair_budget = 0; // step pairs per slot per launch (0: default)
     int fp32_ring_slots = 0;       // cell-table ring slots per slot (0: default 64)
+    int64_t fp64_latency_max = kFp64LatencyMaxTraj;   // latency mode up to this many trajectories
     cudaStream_t side = nullptr;   // post-processing beside running batches (high priority)
     cudaStream_t rd = nullptr;     // result reads of finished jobs, beside running work
     cudaStream_t gside = nullptr;  // side branch captured into batch graphs

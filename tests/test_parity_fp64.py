@@ -45,6 +45,33 @@ def double(steps=120_000, freq=40, **kw):
     return _set(p, kw)
 
 
+@pytest.fixture(scope="module")
+def ctx_thread():
+    # a context whose FP64 jobs never use latency mode
+    c = ldp.Context(0)
+    c.set_fp64_latency(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module", params=["latency", "thread"])
+def ctx(request, ctx_thread):
+    # Every parity case runs twice: small jobs in latency mode (a CTA per
+    # trajectory, the default below 2048 trajectories) and with one
+    # trajectory per thread; both must equal the oracle bit for bit.
+    if request.param == "thread":
+        return ctx_thread
+    c = request.getfixturevalue("ctx_default")
+    return c
+
+
+@pytest.fixture(scope="module")
+def ctx_default():
+    c = ldp.Context(0)
+    yield c
+    c.close()
+
+
 def run_both(ctx, p, seed=1234, lanes=8, ranks=1, slots=256, tick_cap=-1, mode=0, step_cap=0, spl=0, job_id=0):
     p.random_seed = seed
     with ldp.Job(ctx, p, lanes=lanes, ranks=ranks, table_slots=slots, tick_cap=tick_cap, mode=mode,
