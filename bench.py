@@ -48,6 +48,13 @@ FP64_STEPS = 2      # timed passes of the FP64 plain leg (one untimed before)
 # FP64 mean's relative standard error is ~0.2 %.  Its device times also give
 # both paths' throughput on an event-heavy workload.
 ACC_JOB, ACC_NTRAJ, ACC_NSTEPS, ACC_FREQSAVE = 14, 65536, 5_000_000, 2500
+# The reference's own sample run (quick_test): its .inp verbatim (overdamped
+# single barrier, dt 1e-4, TAU 1e-5, all statistics, WRITEX), 4 ranks x 8
+# lanes = 32 trajectories, with NUMBEROFSTEPS scaled from 3e9 to QT_STEPS
+# (and FREQSAVE so that the run keeps >= 1100 frames); the FP64 plain path as
+# the drop-in executable runs it.  The reference took 7.133 min on 4 Xeon
+# ranks for 16 trajectories x 3e9 steps (its executed_job time.log).
+QT_STEPS, QT_FULL_STEPS, QT_REF_S = 30_000_000, 3_000_000_000, 7.133333 * 60
 # DRAM bytes per particle-step of the persistent kernel: 0.0873 B measured by
 # ncu with frames every 100 steps, of which the frames are 8 B per frame
 # (0.0801 B per step); the rest (0.0072 B: retire records, ring) is kept and
@@ -239,6 +246,28 @@ def compare_summaries(a, b):
     return out
 
 
+def quick_test_leg(ldp, ctx, job_id0):
+    """The reference's sample (C1) through the FP64 plain path: ns per step
+    of its 32 trajectories and the projected wall time of the full 3e9-step
+    run, beside the reference's recorded time."""
+    p = ldp.params_from_inp(os.path.join(ROOT, "tests", "golden", "inp", "quick_test__2.0_7.2_m1.0_1.00e-05.inp"))
+    p.number_of_steps, p.freq_save, p.random_seed = QT_STEPS, QT_STEPS // 2000, 1234
+    p.write_restart = 0
+    with ldp.Job(ctx, p, lanes=8, ranks=4, job_id=job_id0) as j:
+        ctx.mark(4)
+        j.submit()
+        j.wait()
+        ctx.mark(5)
+        ms = ctx.elapsed_ms(4, 5)
+    ns_step = ms * 1e6 / QT_STEPS
+    return {"workload": "sample_input/quick_test .inp verbatim, 4 ranks x 8 lanes = 32 trajectories, "
+                        f"{QT_STEPS} steps (FREQSAVE {QT_STEPS // 2000})",
+            "ms": ms, "ns_per_step": ns_step, "particle_steps_per_s": 32 * QT_STEPS / (ms * 1e-3),
+            "projected_full_run_s": ns_step * 1e-9 * QT_FULL_STEPS,
+            "reference_full_run_s": QT_REF_S,
+            "reference_note": "16 trajectories x 3e9 steps on 4 Xeon Gold 6136 ranks (executed_job time.log)"}
+
+
 def accuracy_leg(ldp, ctx, job_id0):
     """FP32 batched vs FP64 plain on one job of the mix, sized for a small
     FP64 standard error (outside the timed region; each run's device time is
@@ -397,6 +426,7 @@ def main():
     fp64_ms = rep.max_over_ranks(sum(t64) / len(t64))
     fp64_value = psteps / (fp64_ms * 1e-3)
     accuracy = accuracy_leg(ldp, ctx, job_id0)
+    quick_test = quick_test_leg(ldp, ctx, job_id0)
 
     # ---- end to end through the C ABI: host params in, host results out ----
     e2e_t = []
@@ -469,6 +499,7 @@ def main():
                                      f"(FP64 jobs side by side on two streams), {FP64_STEPS} timed passes"},
             "fp32_over_fp64": value / (fp64_value * world),
             "accuracy_vs_fp64": accuracy,
+            "quick_test_fp64": quick_test,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches / max(1, args.steps)),
