@@ -268,6 +268,27 @@ def quick_test_leg(ldp, ctx, job_id0):
             "reference_note": "16 trajectories x 3e9 steps on 4 Xeon Gold 6136 ranks (executed_job time.log)"}
 
 
+# Serving leg: SERVE_JOBS jobs of the serving workload (types single/double x
+# over/underdamped, 2^U[10,18] trajectories, 24000 steps, parameters from the
+# precision / batching / scan ranges): capacity with every job submitted at
+# once, then Poisson streams at 50 % and 80 % of it.  The full workload is
+# 10^4 jobs (langevindynamicsforpcp_b200.serve); this many fit the bench.
+SERVE_JOBS = 1000
+
+
+def serving_leg(device):
+    """p50 / p99 job latency of the serving loop (its own context)."""
+    from langevindynamicsforpcp_b200 import serve
+    r = serve.measure(jobs=SERVE_JOBS, loads=(0.5, 0.8), isolated_sample=24, device=device)
+    out = {"workload": r["workload"], "capacity": r["capacity"], "isolated": r["isolated"], "loads": {}}
+    for load, v in r["loads"].items():
+        out["loads"][load] = {k: v[k] for k in ("rate_jobs_per_s", "p50_latency_s", "p99_latency_s",
+                                                "p50_over_isolated", "p99_over_isolated",
+                                                "p99_latency_over_p99_isolated", "particle_steps_per_s",
+                                                "by_trajectory_count")}
+    return out
+
+
 def accuracy_leg(ldp, ctx, job_id0):
     """FP32 batched vs FP64 plain on one job of the mix, sized for a small
     FP64 standard error (outside the timed region; each run's device time is
@@ -331,6 +352,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="2 jobs x 16384 trajectories (for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (profiling cases)")
     ap.add_argument("--nsteps", type=int, default=None, help="steps per trajectory (profiling cases)")
     ap.add_argument("--njobs", type=int, default=None, help="jobs per batch (profiling cases)")
     ap.add_argument("--freqsave", type=int, default=None, help="steps between frames (profiling cases)")
@@ -427,6 +449,7 @@ def main():
     fp64_value = psteps / (fp64_ms * 1e-3)
     accuracy = accuracy_leg(ldp, ctx, job_id0)
     quick_test = quick_test_leg(ldp, ctx, job_id0)
+    serving = serving_leg(local) if not args.no_serving else None
 
     # ---- end to end through the C ABI: host params in, host results out ----
     e2e_t = []
@@ -500,6 +523,7 @@ def main():
             "fp32_over_fp64": value / (fp64_value * world),
             "accuracy_vs_fp64": accuracy,
             "quick_test_fp64": quick_test,
+            "serving": serving,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches / max(1, args.steps)),

@@ -195,20 +195,18 @@ def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 
     return lat
 
 
-def main(argv=None):
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--jobs", type=int, default=10000)
-    ap.add_argument("--exp-lo", type=float, default=10)
-    ap.add_argument("--exp-hi", type=float, default=18)
-    ap.add_argument("--steps", type=int, default=24000)
-    ap.add_argument("--loads", type=float, nargs="+", default=[0.5, 0.8])
-    ap.add_argument("--isolated-sample", type=int, default=24)
-    a = ap.parse_args(argv)
+def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: int = 24000, loads=(0.5, 0.8),
+            isolated_sample: int = 24, device: int = 0) -> dict:
+    """Capacity (every job submitted at once), isolated solve times and, per
+    offered load (a fraction of that capacity), the latency distribution of
+    a Poisson stream of the serving workload's jobs."""
+    a = argparse.Namespace(jobs=jobs, exp_lo=exp_lo, exp_hi=exp_hi, steps=steps, loads=list(loads),
+                           isolated_sample=isolated_sample)
     work = serving_workload(a.jobs, exp_lo=a.exp_lo, exp_hi=a.exp_hi, steps=a.steps)
     psteps = float(sum(n for _, n, _ in work)) * a.steps
     out = {"workload": f"serving: {a.jobs} jobs, types single/double x over/underdamped, "
                        f"2^U[{a.exp_lo:g},{a.exp_hi:g}] trajectories, {a.steps} steps", "loads": {}}
-    with Context(0) as ctx, Server(ctx) as srv:
+    with Context(device) as ctx, Server(ctx) as srv:
         # warm-up (first launches of each kernel, first use of each queue)
         run_stream(srv, serving_workload(32, seed=99, exp_lo=a.exp_lo, exp_hi=a.exp_hi, steps=a.steps),
                    np.zeros(32))
@@ -271,7 +269,19 @@ def main(argv=None):
                                 "isolated_s": isolated(int(i)), "stages_s": [float(x) for x in stg[i]]}
                                for i in np.argsort(-ratio)[:4]]}
         out["isolated"] = {"jobs": len(iso), "median_s": float(np.median(list(iso.values())))}
-    print(json.dumps(out))
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--jobs", type=int, default=10000)
+    ap.add_argument("--exp-lo", type=float, default=10)
+    ap.add_argument("--exp-hi", type=float, default=18)
+    ap.add_argument("--steps", type=int, default=24000)
+    ap.add_argument("--loads", type=float, nargs="+", default=[0.5, 0.8])
+    ap.add_argument("--isolated-sample", type=int, default=24)
+    a = ap.parse_args(argv)
+    print(json.dumps(measure(a.jobs, a.exp_lo, a.exp_hi, a.steps, a.loads, a.isolated_sample)))
 
 
 if __name__ == "__main__":
