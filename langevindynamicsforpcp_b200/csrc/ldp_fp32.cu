@@ -738,10 +738,14 @@ __device__ __forceinline__ int light_step(const JobF* jobs, const SlotsDev& S, R
 #define LDP_FP32_MIN_BLOCKS 3
 #endif
 
+// The persistent loop of one model type for the calling warp: its slots'
+// trajectories (and new ones claimed from queue q) for up to quad_budget
+// blocks of four steps.  Returns the blocks run; *drained is set when it
+// stopped early because every lane of the warp was idle and the queue had
+// nothing left for it.  Slot state is loaded at entry and saved at exit.
 template <bool DBL, bool OVER>
-__global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kernel(
-    const __grid_constant__ QueueDev q, const __grid_constant__ SlotsDev S, uint32_t quad_budget) {
-    __shared__ RareSm sm;
+__device__ __forceinline__ uint32_t persistent_run(const QueueDev& q, const SlotsDev& S, RareSm& sm,
+                                                   uint32_t quad_budget, bool* drained) {
     const int t = threadIdx.x;
     const int64_t slot = (int64_t)blockIdx.x * blockDim.x + t;
     const unsigned lane = t & 31u;
@@ -808,7 +812,8 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
     }
 
     bool dry = false;   // the queue had nothing left for this warp
-    for (uint32_t it = 0; it < quad_budget; ++it) {
+    uint32_t it = 0;
+    for (; it < quad_budget; ++it) {
         // ---- warp-aggregated refill of idle lanes ----
         const unsigned idle = __ballot_sync(kFull, job < 0);
         if (__builtin_expect(idle != 0, 0)) {
@@ -858,7 +863,10 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
                 }
             }
             if (__all_sync(kFull, job < 0)) {
-                if (dry || m == 0) break;
+                if (dry || m == 0) {
+                    *drained = true;
+                    break;
+                }
                 continue;
             }
             if (job < 0) continue;
@@ -914,7 +922,7 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         ++j;
     }
 
-    if (slot >= S.nslots) return;
+    if (slot >= S.nslots) return it;
     S.job[slot] = job;
     if (job >= 0) {
         const JobF& J = q.jobs[job];
@@ -942,6 +950,72 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
         J.tpt_last[traj] = sm.tpt[t];
         J.tpt2_last[traj] = sm.tpt2[t];
     }
+    return it;
+}
+
+template <bool DBL, bool OVER>
+__global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kernel(
+    const __grid_constant__ QueueDev q, const __grid_constant__ SlotsDev S, uint32_t quad_budget) {
+    __shared__ RareSm sm;
+    bool drained = false;
+    persistent_run<DBL, OVER>(q, S, sm, quad_budget, &drained);
+}
+
+// All four model types in one persistent launch (the serving loop's).  A
+// warp serves one type at a time -- a warp-uniform switch over the four
+// instantiated loops -- with every lane's trajectory from that type's queue;
+// when all its lanes are idle and that queue is dry it takes the next type
+// with unclaimed items (round robin from a start spread over warps), so no
+// type's work waits for another type's launch.  The warp's type is kept
+// across launches in wtype (-1: none).  A warp ends its launch when the
+// budget is spent, no queue has work, or eight type changes in a row found
+// nothing to claim (claims raced away by other warps).
+template <int kUnused>
+__global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_mixed_kernel(const __grid_constant__ MixedDev m,
+                                                                               uint32_t quad_budget) {
+    __shared__ RareSm sm;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int type = m.wtype[w];
+    uint32_t left = quad_budget;
+    int empty_picks = 0;
+    while (left > 0) {
+        if (type < 0) {
+            int pick = -1;
+            if ((threadIdx.x & 31) == 0) {
+                const int start = (int)(w & 3);
+                for (int k = 0; k < 4; ++k) {
+                    const int tt = (start + k) & 3;
+                    const unsigned long long h = *(volatile const unsigned long long*)m.q[tt].head;
+                    const unsigned long long tl = *(volatile const unsigned long long*)m.q[tt].tail;
+                    if (h < tl) {
+                        pick = tt;
+                        break;
+                    }
+                }
+            }
+            pick = __shfl_sync(kFull, pick, 0);
+            if (pick < 0) break;
+            type = pick;
+        }
+        bool drained = false;
+        uint32_t used;
+        switch (type) {
+            case 0: used = persistent_run<false, false>(m.q[0], m.S, sm, left, &drained); break;
+            case 1: used = persistent_run<false, true>(m.q[1], m.S, sm, left, &drained); break;
+            case 2: used = persistent_run<true, false>(m.q[2], m.S, sm, left, &drained); break;
+            default: used = persistent_run<true, true>(m.q[3], m.S, sm, left, &drained); break;
+        }
+        left -= (used < left) ? used : left;
+        if (drained) {
+            type = -1;
+            if (used == 0) {
+                if (++empty_picks >= 8) break;
+            } else {
+                empty_picks = 0;
+            }
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && w < m.nwarps) m.wtype[w] = type;
 }
 
 // Publishes item ranges [.., new_tail): clamps the head (claims may have run
@@ -978,6 +1052,21 @@ int fp32_blocks_per_sm(bool dbl, bool over, int block) {
     else e = over ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp32_persistent_kernel<false, true>, block, 0)
                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp32_persistent_kernel<false, false>, block, 0);
     return e == cudaSuccess ? n : 0;
+}
+
+int fp32_mixed_blocks_per_sm(int block) {
+    int n = 0;
+    cudaError_t e = cudaFuncSetAttribute(fp32_mixed_kernel<0>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp32_mixed_kernel<0>, block, 0);
+    return e == cudaSuccess ? n : 0;
+}
+
+int launch_fp32_mixed(const MixedDev& m, uint32_t pair_budget, int grid, int block, void* stream) {
+    const uint32_t quad_budget = pair_budget > 1 ? pair_budget / 2 : 1;
+    if (block != 256 || (int64_t)grid * block > m.S.nslots) return (int)cudaErrorInvalidValue;
+    fp32_mixed_kernel<0><<<grid, block, 0, (cudaStream_t)stream>>>(m, quad_budget);
+    return (int)cudaGetLastError();
 }
 
 int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint32_t pair_budget, int grid,

@@ -107,11 +107,24 @@ struct SlotsDev {
     int32_t ring_slots;
 };
 
+// The four model types' queues and one set of slots shared by them, for the
+// mixed persistent kernel (the serving loop's launches); wtype[w] is the
+// type warp w serves (-1: none).
+struct MixedDev {
+    QueueDev q[4];
+    SlotsDev S;
+    int32_t* wtype;
+    int64_t nwarps;
+};
+
 // Appends published work: clamps head to the old tail, sets tail and nranges.
 int launch_fp32_publish(const QueueDev& q, unsigned long long new_tail, int32_t new_nranges, void* stream);
 // Resident blocks per SM of the persistent kernel (0 on error).
 int fp32_blocks_per_sm(bool dbl, bool over, int block);
 int launch_fp32_persistent(bool dbl, bool over, const QueueDev& q, const SlotsDev& s, uint32_t pair_budget,
                            int grid, int block, void* stream);
+// Resident 256-thread blocks per SM of the mixed kernel, and its launch.
+int fp32_mixed_blocks_per_sm(int block);
+int launch_fp32_mixed(const MixedDev& m, uint32_t pair_budget, int grid, int block, void* stream);
 
 }  // namespace ldp

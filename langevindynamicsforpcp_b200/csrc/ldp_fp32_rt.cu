@@ -45,6 +45,12 @@ struct Fp32Queue {
 
 struct Fp32Runtime {
     Fp32Queue q[4];
+    // mixed launches (serving): one set of slots for all four queues, the
+    // type each warp serves
+    SlotsDev mixed{};
+    void* mixed_mem = nullptr;
+    int32_t* wtype = nullptr;
+    int mixed_grid = 0;
 };
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -57,6 +63,45 @@ static int64_t* stage(Fp32Queue& Q) {
     cudaEventSynchronize(Q.stage_ev[si]);
     Q.stage_last = si;
     return Q.h_stage + (size_t)si * (4096 / sizeof(int64_t));
+}
+
+// One set of persistent slots (their state between launches): nslots
+// slots with R cell-table ring entries each, every slot empty.
+static int slots_init(int64_t nslots, int R, SlotsDev* Sp, void** mem) {
+    size_t sb = al256(sizeof(int32_t) * nslots) * 6 + al256(sizeof(int64_t) * nslots) * 7 +
+                al256(sizeof(float) * nslots) * 2 + al256(sizeof(longlong2) * (size_t)R * nslots) +
+                al256(sizeof(unsigned long long));
+    cudaError_t e = cudaMalloc(mem, sb);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaMemset(*mem, 0, sb);
+    if (e != cudaSuccess) return (int)e;
+    char* a = (char*)*mem;
+    size_t o = 0;
+    SlotsDev& S = *Sp;
+    S.nslots = nslots;
+    S.ring_slots = R;
+    S.job = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.cell = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.st = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.ckey = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.cgw = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.fidx = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
+    S.nxf = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.nflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.traj = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.step = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.cflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.sc1 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.since = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
+    S.xp = (float*)(a + o); o += al256(sizeof(float) * nslots);
+    S.rv = (float*)(a + o); o += al256(sizeof(float) * nslots);
+    S.ring = (longlong2*)(a + o); o += al256(sizeof(longlong2) * (size_t)R * nslots);
+    S.retired = (unsigned long long*)(a + o);
+    // every slot starts empty
+    std::vector<int32_t> neg((size_t)nslots, -1);
+    e = cudaMemcpy(S.job, neg.data(), sizeof(int32_t) * nslots, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return (int)e;
+    return 0;
 }
 
 static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
@@ -89,40 +134,7 @@ static int queue_init(ldp_ctx* ctx, Fp32Queue& Q, int type, int ring_slots) {
     Q.q.nranges = (int32_t*)(a + o); o += al256(sizeof(int32_t));
     Q.q.jobs = (JobF*)(a + o); o += al256(sizeof(JobF) * kFp32MaxJobs);
     Q.rem = (unsigned long long*)(a + o);
-    // slots
-    const int R = ring_slots;
-    size_t sb = al256(sizeof(int32_t) * nslots) * 6 + al256(sizeof(int64_t) * nslots) * 7 +
-                al256(sizeof(float) * nslots) * 2 + al256(sizeof(longlong2) * (size_t)R * nslots) +
-                al256(sizeof(unsigned long long));
-    e = cudaMalloc(&Q.smem, sb);
-    if (e != cudaSuccess) return (int)e;
-    e = cudaMemset(Q.smem, 0, sb);
-    if (e != cudaSuccess) return (int)e;
-    a = (char*)Q.smem;
-    o = 0;
-    SlotsDev& S = Q.s;
-    S.nslots = nslots;
-    S.ring_slots = R;
-    S.job = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
-    S.cell = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
-    S.st = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
-    S.ckey = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
-    S.cgw = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
-    S.fidx = (int32_t*)(a + o); o += al256(sizeof(int32_t) * nslots);
-    S.nxf = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.nflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.traj = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.step = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.cflip = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.sc1 = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.since = (int64_t*)(a + o); o += al256(sizeof(int64_t) * nslots);
-    S.xp = (float*)(a + o); o += al256(sizeof(float) * nslots);
-    S.rv = (float*)(a + o); o += al256(sizeof(float) * nslots);
-    S.ring = (longlong2*)(a + o); o += al256(sizeof(longlong2) * (size_t)R * nslots);
-    S.retired = (unsigned long long*)(a + o);
-    // every slot starts empty
-    std::vector<int32_t> neg((size_t)nslots, -1);
-    e = cudaMemcpy(S.job, neg.data(), sizeof(int32_t) * nslots, cudaMemcpyHostToDevice);
+    e = (cudaError_t)slots_init(nslots, ring_slots, &Q.s, &Q.smem);
     if (e != cudaSuccess) return (int)e;
     e = cudaMallocHost((void**)&Q.h_stage, 4096 * Fp32Queue::kStageSlots);
     if (e != cudaSuccess) return (int)e;
@@ -244,6 +256,41 @@ int fp32_launch_type(ldp_ctx* ctx, int type, uint32_t pair_budget, cudaStream_t 
     if (!Q.ready) return 0;
     return launch_fp32_persistent(type >= 2, (type & 1) != 0, Q.q, Q.s, pair_budget, Q.grid, Q.block, st);
 }
+
+// One persistent launch over all four model types' queues (serving): the
+// queues are created if they were not, and the mixed kernel's slots on
+// first use.
+int fp32_launch_mixed(ldp_ctx* ctx, uint32_t pair_budget, cudaStream_t st) {
+    if (!ctx->fp32) ctx->fp32 = new Fp32Runtime();
+    Fp32Runtime& R = *ctx->fp32;
+    const int ring = ctx->fp32_ring_slots ? ctx->fp32_ring_slots : 64;
+    for (int t = 0; t < 4; ++t) {
+        const int e = queue_init(ctx, R.q[t], t, ring);
+        if (e) return e;
+    }
+    if (!R.mixed_mem) {
+        const int block = 256;
+        int bps = fp32_mixed_blocks_per_sm(block);
+        if (ctx->fp32_blocks_per_sm) bps = std::min(bps, ctx->fp32_blocks_per_sm);
+        bps = std::max(bps, 1);
+        R.mixed_grid = ctx->sm_count * bps;
+        const int64_t nslots = (int64_t)R.mixed_grid * block;
+        int e = slots_init(nslots, ring, &R.mixed, &R.mixed_mem);
+        if (e) return e;
+        cudaError_t ce = cudaMalloc((void**)&R.wtype, sizeof(int32_t) * (size_t)(nslots / 32));
+        if (ce == cudaSuccess) ce = cudaMemset(R.wtype, 0xff, sizeof(int32_t) * (size_t)(nslots / 32));   // -1
+        if (ce != cudaSuccess) return (int)ce;
+    }
+    MixedDev m;
+    for (int t = 0; t < 4; ++t) m.q[t] = R.q[t].q;
+    m.S = R.mixed;
+    m.wtype = R.wtype;
+    m.nwarps = R.mixed.nslots / 32;
+    return launch_fp32_mixed(m, pair_budget, R.mixed_grid, 256, st);
+}
+
+// Slots of the mixed launches (0 before the first).
+int64_t fp32_mixed_slots(ldp_ctx* ctx) { return ctx->fp32 ? ctx->fp32->mixed.nslots : 0; }
 
 // Asynchronous copy of a queue's per-slot remaining counters and of its
 // claimed-items count (serving).
@@ -413,6 +460,8 @@ void fp32_release(ldp_job* job) {
 
 void fp32_destroy_runtime(ldp_ctx* ctx) {
     if (!ctx->fp32) return;
+    if (ctx->fp32->mixed_mem) cudaFree(ctx->fp32->mixed_mem);
+    if (ctx->fp32->wtype) cudaFree(ctx->fp32->wtype);
     for (auto& Q : ctx->fp32->q) {
         if (Q.qmem) cudaFree(Q.qmem);
         if (Q.smem) cudaFree(Q.smem);

@@ -95,6 +95,9 @@ int fp32_launch_bound(ldp_ctx* ctx, int type, double total_pairs, double max_pai
 int fp32_remaining(ldp_job* job, unsigned long long* rem);
 int fp32_type_of(const ldp_job* job);
 int fp32_launch_type(ldp_ctx* ctx, int type, uint32_t pair_budget, cudaStream_t st);
+// One launch of the mixed kernel over all four types' queues (serving).
+int fp32_launch_mixed(ldp_ctx* ctx, uint32_t pair_budget, cudaStream_t st);
+int64_t fp32_mixed_slots(ldp_ctx* ctx);
 int fp32_copy_remaining(ldp_ctx* ctx, int type, unsigned long long* host, unsigned long long* head,
                         cudaStream_t st);
 int64_t fp32_nslots(ldp_ctx* ctx, int type);

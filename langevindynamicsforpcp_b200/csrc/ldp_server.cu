@@ -15,9 +15,10 @@
 //     (shortest remaining first): a small job that arrives while large ones
 //     run starts within one chunk, instead of after every earlier job;
 //  3. keeps up to `max_inflight` short persistent launches (pair budget
-//     `pair_budget`) in flight per model type with active jobs, each type on
-//     its own stream, so the types share the GPU and newly published work is
-//     reached within one launch;
+//     `pair_budget`) in flight while any job is active, each over all four
+//     model types' queues (a warp serves one type at a time and moves to
+//     another type with work when its lanes are idle), so the types share
+//     every launch and newly published work is reached within one launch;
 //  4. reads every queue's per-job "trajectories not yet retired" counters
 //     (and its claimed-items count) with one asynchronous copy, and for each
 //     job whose counter reached zero enqueues its post-processing (event
@@ -76,7 +77,8 @@ struct ldp_server {
     uint32_t pair_budget = 0;
     int max_inflight = 2;
     cudaStream_t side = nullptr;         // post-processing
-    cudaStream_t qs[4] = {};             // one per model type: publication, launches, counter copies
+    cudaStream_t q = nullptr;            // the queues' work: registration, publication, launches, counter copies
+    cudaStream_t qs[4] = {};             // per model type: all q (one stream orders every queue's work)
     unsigned long long head_seen[4] = {};
     std::mutex mu;                       // guards pending and all
     std::deque<Entry*> pending;
@@ -170,8 +172,9 @@ extern "C" ldp_status ldp_server_create(ldp_ctx* ctx, const ldp_server_opts* o, 
         // the queue's counters, then its claimed-items count
         e = cudaMallocHost((void**)&s->h_rem[t], sizeof(unsigned long long) * (ldp::kFp32MaxJobs + 1));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->rem_ev[t], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->qs[t], cudaStreamNonBlocking, lo_prio);
     }
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->q, cudaStreamNonBlocking, lo_prio);
+    for (int t = 0; t < 4; ++t) s->qs[t] = s->q;
     if (e != cudaSuccess) {
         ldp_server_destroy(s);
         ldp_set_error(ctx, "server set-up failed: %s", cudaGetErrorString(e));
@@ -339,22 +342,24 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
 
     s->phase(2, tp);
 
-    // 3. persistent launches of every type with work
-    for (int t = 0; t < 4; ++t) {
-        auto& q = s->inflight[t];
+    // 3. persistent launches: each covers every model type's queue (a warp
+    //    serves one type at a time and moves to another with work when its
+    //    lanes are idle), so no type waits behind another type's launch
+    {
+        auto& q = s->inflight[0];
         while (!q.empty() && cudaEventQuery(q.front()) == cudaSuccess) {
             s->pool.push_back(q.front());
             q.pop_front();
         }
-        if (!active[t]) continue;
-        while ((int)q.size() < s->max_inflight) {
-            const int e = ldp::fp32_launch_type(ctx, t, s->pair_budget, s->qs[t]);
+        const bool any = active[0] || active[1] || active[2] || active[3];
+        while (any && (int)q.size() < s->max_inflight) {
+            const int e = ldp::fp32_launch_mixed(ctx, s->pair_budget, s->q);
             if (e) return fail(s, "persistent launch", (cudaError_t)e);
             ++s->launches;
             cudaEvent_t ev = s->get_event();
             if (!ev) return fail(s, "event creation", cudaErrorMemoryAllocation);
             q.push_back(ev);
-            const cudaError_t ce = cudaEventRecord(ev, s->qs[t]);
+            const cudaError_t ce = cudaEventRecord(ev, s->q);
             if (ce != cudaSuccess) return fail(s, "launch event", ce);
         }
     }
@@ -512,8 +517,7 @@ extern "C" void ldp_server_destroy(ldp_server* s) {
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
     if (s->side) cudaStreamSynchronize(s->side);
-    for (int t = 0; t < 4; ++t)
-        if (s->qs[t]) cudaStreamSynchronize(s->qs[t]);
+    if (s->q) cudaStreamSynchronize(s->q);
     {
         // Jobs never admitted are dropped; jobs still integrating hold queue
         // slots until their trajectories retired, so the loop runs on until
@@ -524,7 +528,7 @@ extern "C" void ldp_server_destroy(ldp_server* s) {
     for (int guard = 0; guard < 100000 && (!s->running.empty() || !s->finishing.empty()); ++guard) {
         if (ldp_server_step(s, nullptr) != LDP_OK) break;
         cudaStreamSynchronize(s->side);
-        for (int t = 0; t < 4; ++t) cudaStreamSynchronize(s->qs[t]);
+        if (s->q) cudaStreamSynchronize(s->q);
     }
     for (auto& kv : s->all) {
         if (kv.second->fin) cudaEventDestroy(kv.second->fin);
@@ -539,7 +543,6 @@ extern "C" void ldp_server_destroy(ldp_server* s) {
     for (cudaEvent_t e : s->pool) cudaEventDestroy(e);
     if (s->region) cudaFree(s->region);
     if (s->side) cudaStreamDestroy(s->side);
-    for (int t = 0; t < 4; ++t)
-        if (s->qs[t]) cudaStreamDestroy(s->qs[t]);
+    if (s->q) cudaStreamDestroy(s->q);
     delete s;
 }
