@@ -458,6 +458,25 @@ typedef struct ldp_restart_summary {
     int32_t min_id[2];        /* first cell index of each table              */
 } ldp_restart_summary;
 ldp_status  ldp_job_restore(ldp_job *job, const char *input_base);
+/*
+ * Continuation of FP32 batched runs (the chaining the reference does with
+ * WRITERESTART / READRESTART, src/langevinDynamicsSingleBarrier.h:1048-1275,
+ * whose .restart files hold per-event lists this path does not keep).
+ * ldp_job_keep_state, before ldp_submit: the job keeps every trajectory's
+ * state at its last step (~(40 + 16 x ring slots) device bytes per
+ * trajectory).  ldp_job_save_state, after the run: writes that state, the
+ * counts, duration sums, frames and waiting-time ticks to a file of this
+ * library.  ldp_job_load_state, before ldp_submit: loads such a file into a
+ * job of the same parameters, layout, RANDOMSEED and job id whose
+ * NUMBEROFPREVIOUSSTEPS equals the steps the file holds (a multiple of 4);
+ * NUMBEROFSTEPS more steps follow and the job can be saved again.  The
+ * random streams are keyed by absolute step, so a chained run equals the
+ * uninterrupted one bit for bit.  Fixed-step mode only.  No reference
+ * counterpart for the file itself.
+ */
+ldp_status  ldp_job_keep_state(ldp_job *job);
+ldp_status  ldp_job_save_state(ldp_job *job, const char *path);
+ldp_status  ldp_job_load_state(ldp_job *job, const char *path);
 ldp_status  ldp_job_save_restart(ldp_job *job, const char *output_base);
 /* One file: its summary and, optionally, the per-lane counts and sums a
  * job restored from it starts with ([LDP_NCOUNT][lanes], [LDP_NSUM][lanes]).

@@ -150,6 +150,23 @@ class Job:
         _check(L.lib().ldp_job_save_restart(self.handle, output_base.encode()), self.ctx)
         return self
 
+    def keep_state(self) -> "Job":
+        """FP32 batched: keep every trajectory's state at its last step, so
+        that save_state can write it (before submission)."""
+        _check(L.lib().ldp_job_keep_state(self.handle), self.ctx)
+        return self
+
+    def save_state(self, path: str) -> "Job":
+        """FP32 batched: writes the kept state (ldp_job_save_state)."""
+        _check(L.lib().ldp_job_save_state(self.handle, path.encode()), self.ctx)
+        return self
+
+    def load_state(self, path: str) -> "Job":
+        """FP32 batched: continues from a saved state (before submission);
+        NUMBEROFPREVIOUSSTEPS must equal its step count."""
+        _check(L.lib().ldp_job_load_state(self.handle, path.encode()), self.ctx)
+        return self
+
     # -- introspection -----------------------------------------------------
     @property
     def info(self) -> L.JobInfo:

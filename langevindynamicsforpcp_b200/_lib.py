@@ -166,6 +166,9 @@ SIGNATURES = {
     "ldp_server_info_get": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
     "ldp_server_destroy": (None, [C.c_void_p]),
     "ldp_ctx_set_fp64_latency": (C.c_int, [C.c_void_p, C.c_int64]),
+    "ldp_job_keep_state": (C.c_int, [C.c_void_p]),
+    "ldp_job_save_state": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ldp_job_load_state": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ldp_inp_print_values": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ldp_integrate_fp64_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(JobOpts), C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),

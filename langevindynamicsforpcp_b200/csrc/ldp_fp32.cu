@@ -232,6 +232,39 @@ __device__ __noinline__ void f_start(const JobF* Jp, longlong2* ring, int64_t ns
                                      int* sw) {
     const JobF& J = *Jp;
     const uint32_t g = traj + J.g0;   // the trajectory's random streams
+    if (J.resume) {
+        // Continue from the state kept at step S = step0 - 1: the ring, the
+        // hot state, the statistics clocks; the state-1 steps counted so far
+        // complete, a state-1 run going on restarting at S + 1 (the same
+        // total); frames continue after frame S / FREQSAVE.
+        const int64_t n = J.ntraj;
+        for (int r = 0; r < ring_slots; ++r) ring[(int64_t)r * nslots + slot] = J.ck_ring[(int64_t)r * n + traj];
+        // a trajectory frozen as non-finite stays so (its first step retires it)
+        *xp = (J.counts[(int64_t)LDP_C_FLAGS * n + traj] & LDP_FLAG_NONFINITE) ? __int_as_float(0x7fc00000)
+                                                                                : J.ck_xp[traj];
+        *rv = J.ck_rv[traj];
+        *cell = J.ck_cell[traj];
+        *sw = J.ck_sw[traj];
+        *state = J.state_final[traj];
+        sm->bits[t] = (uint32_t)J.bits[traj];
+        sm->init0[t] = J.init_idx0[traj];
+        sm->idx2[t] = J.idx2_0[traj];
+        sm->tpt2w[t] = J.tpt2_well[traj];
+        sm->ckey[t] = J.ck_ckey[traj];
+        sm->cflip[t] = J.ck_cflip[traj];
+        sm->nflip[t] = J.ck_nflip[traj];
+        sm->fpt[t] = J.fpt_last[traj];
+        sm->fpt2[t] = J.fpt2_last[traj];
+        sm->tpt[t] = J.tpt_last[traj];
+        sm->tpt2[t] = J.tpt2_last[traj];
+        sm->cgw[t] = INT32_MIN;
+        const uint64_t S0 = J.step0 - 1, fs = J.freq_save;
+        sm->fidx[t] = (int)(S0 / fs) + 1;
+        sm->nxf[t] = (long long)((S0 / fs + 1) * fs);
+        sm->sc1[t] = J.counts[(int64_t)LDP_C_STATE1 * n + traj];
+        sm->since[t] = (long long)J.step0;
+        return;
+    }
     for (int r = 0; r < ring_slots; ++r) ring[(int64_t)r * nslots + slot] = make_longlong2((long long)INT64_MIN, 0);
     const double red = J.x0 * J.invL;
     const int c = (int)rint(red);
@@ -346,6 +379,33 @@ __device__ __forceinline__ void retire_lane(const JobF& J, unsigned long long* r
     f_retire(&J, retired, sm.traj[t], done, sc1, sm.cell[t], xp, OVER ? 0.0f : v, state, flags);
 }
 
+// Keeps the continuation state of a trajectory that completed its last
+// step (see JobF::ck_*); rv: the velocity after the step (underdamped) or
+// the step's random force (overdamped).
+__device__ __noinline__ void f_keep_state(const JobF* Jp, const SlotsDev* Sp, const RareSm* smp, int t, int64_t slot,
+                                          uint32_t traj, float xp, float rv, int cell, int sw) {
+    const JobF& J = *Jp;
+    const SlotsDev& S = *Sp;
+    const RareSm& sm = *smp;
+    const int64_t n = J.ntraj;
+    J.ck_xp[traj] = xp;
+    J.ck_rv[traj] = rv;
+    J.ck_cell[traj] = cell;
+    J.ck_sw[traj] = sw;
+    J.ck_ckey[traj] = sm.ckey[t];
+    J.ck_cflip[traj] = sm.cflip[t];
+    J.ck_nflip[traj] = sm.nflip[t];
+    for (int r = 0; r < S.ring_slots; ++r) J.ck_ring[(int64_t)r * n + traj] = S.ring[(int64_t)r * S.nslots + slot];
+    J.bits[traj] = (int32_t)sm.bits[t];
+    J.init_idx0[traj] = sm.init0[t];
+    J.idx2_0[traj] = sm.idx2[t];
+    J.tpt2_well[traj] = sm.tpt2w[t];
+    J.fpt_last[traj] = sm.fpt[t];
+    J.fpt2_last[traj] = sm.fpt2[t];
+    J.tpt_last[traj] = sm.tpt[t];
+    J.tpt2_last[traj] = sm.tpt2[t];
+}
+
 // The general step s of one lane (position already advanced):
 // the FP64 step order of ldp_fp64.cu from the index update on.  Out of line,
 // on the lane state in shared memory, so that the hot loop's registers do
@@ -370,6 +430,7 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     auto retire = [&](uint64_t done, float v, uint32_t flags) {
         sm.cell[t] = cell;
         sm.state[t] = state;
+        if (J.ck_xp && !flags && done == J.nsteps) f_keep_state(&J, &S, &sm, t, slot, traj, xp, OVER ? rv : v, cell, sw);
         retire_lane<OVER>(J, S.retired, sm, t, done, xp, v, flags);
         sm.job[t] = -1;
         sm.lo[t] = -kInf;
@@ -849,7 +910,7 @@ __device__ __forceinline__ uint32_t persistent_run(const QueueDev& q, const Slot
                         f_start<DBL, OVER>(Jn, S.ring, S.nslots, S.ring_slots, slot, traj, &sm, t, &xp, &rv,
                                            &sm.cell[t], &sm.state[t], &sm.sw[t]);
                         sm.job[t] = job;
-                        bind(traj, 1);
+                        bind(traj, Jn->step0);
                         if (Jn->nsteps == 0) {
                             retire_lane<OVER>(*Jn, S.retired, sm, t, 0, xp, rv, 0);
                             job = -1;

@@ -74,6 +74,18 @@ struct JobF {
     int64_t* cg_last;    // [LDP_MAX_CG][ntraj]
     int32_t* cg_well;    // [LDP_MAX_CG][ntraj]
     unsigned long long* remaining;   // trajectories of this job not yet retired
+    // Continuation state at a trajectory's last step (kept when ck_xp is set:
+    // ldp_job_keep_state), and the resume of a job continuing from it
+    // (resume: ldp_job_load_state): position, velocity (underdamped) or the
+    // previous random force (overdamped), cell, slot word (local barrier,
+    // cache, eviction), the cached cell and its pending flip, the current
+    // barrier's pending flip, the cell-table ring [ring slots][ntraj].
+    float *ck_xp, *ck_rv;
+    int32_t *ck_cell, *ck_sw, *ck_ckey;
+    int64_t *ck_cflip, *ck_nflip;
+    longlong2* ck_ring;
+    uint64_t step0;      // the job's first step (1; S + 1 after S previous steps)
+    int32_t resume, pad3;
 };
 
 // A work queue: published item ranges (job index, trajectory count) with

@@ -211,7 +211,10 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
     J->xbd[0] = k.xb[0]; J->xbd[1] = k.xb[1]; J->lo0d = k.lo0; J->hi1d = k.hi1; J->xcd = k.xc;
     J->T_eq = k.T_eq; J->T_as[0] = k.T_as[0]; J->T_as[1] = k.T_as[1];
     J->ln1m[0] = k.ln1m[0]; J->ln1m[1] = k.ln1m[1];
-    J->nsteps = job->nsteps;
+    // steps are numbered after the previous ones of a continued run
+    J->nsteps = job->steps_before + job->nsteps;
+    J->step0 = job->steps_before + 1;
+    J->resume = job->fp32_resume ? 1 : 0;
     J->freq_save = k.freq_save;
     J->nframe = k.nframe;
     J->tick_cap = job->o.tick_cap;
@@ -237,6 +240,9 @@ static void fill_jobf(const ldp_job* job, JobF* J) {
     J->cg_well = b + 5 * n;
     J->cg_last = S.cg_well;   // int64 [ncg][n]
     J->remaining = nullptr;   // the queue's counter of the job's slot, set at registration
+    J->ck_xp = job->ck_xp; J->ck_rv = job->ck_rv; J->ck_cell = job->ck_cell; J->ck_sw = job->ck_sw;
+    J->ck_ckey = job->ck_ckey; J->ck_cflip = job->ck_cflip; J->ck_nflip = job->ck_nflip;
+    J->ck_ring = (longlong2*)job->ck_ring;
 }
 
 int fp32_type_of(const ldp_job* job) { return (job->k.dbl ? 2 : 0) + (job->k.over ? 1 : 0); }

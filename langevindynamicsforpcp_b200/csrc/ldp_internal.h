@@ -79,6 +79,14 @@ struct ldp_job {
     double wall_start = 0.0;
     bool restored = false;       // state loaded by ldp_job_restore
     uint64_t steps_before = 0;   // steps the restart files held
+    // FP32 batched continuation (ldp_job_keep_state / ldp_job_load_state)
+    bool keep_state = false;     // keep each trajectory's state at its last step
+    bool fp32_resume = false;    // continue from a loaded state
+    int ck_ring_slots = 0;       // ring slots of the kept state
+    float *ck_xp = nullptr, *ck_rv = nullptr;
+    int32_t *ck_cell = nullptr, *ck_sw = nullptr, *ck_ckey = nullptr;
+    int64_t *ck_cflip = nullptr, *ck_nflip = nullptr;
+    void* ck_ring = nullptr;
     bool ev_auto = false;        // event_cap / tick_cap chosen by the library
     bool tick_auto = false;
     int64_t particle_steps_done() const;

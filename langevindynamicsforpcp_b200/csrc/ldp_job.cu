@@ -267,8 +267,8 @@ static ldp_status validate(ldp_ctx* ctx, const ldp_params& p, const ldp_job_opts
         return LDP_ERR_INVALID;
     }
     const bool plain = o.precision == LDP_PREC_FP64_PLAIN;
-    if (p.number_of_previous_steps && !(plain && fixed)) {
-        ldp_set_error(ctx, "NUMBEROFPREVIOUSSTEPS (a restart) needs the FP64 plain path in fixed-step mode");
+    if (p.number_of_previous_steps && !fixed) {
+        ldp_set_error(ctx, "NUMBEROFPREVIOUSSTEPS (a continued run) needs fixed-step mode");
         return LDP_ERR_UNSUPPORTED;
     }
     if (o.event_cap > 0 && !(plain && fixed)) {
@@ -326,6 +326,12 @@ static size_t job_arena(ldp_job* job, bool alloc, void* at = nullptr) {
     // FP32 batched extras: integer event-duration sums and 32-bit cell indices.
     const size_t o_ssum = take(f32 ? sizeof(int64_t) * LDP_NSUM * n : 0);
     const size_t o_i32b = take(f32 ? sizeof(int32_t) * (5 + ncg_rows) * n : 0);
+    // FP32 continuation state (ldp_job_keep_state)
+    const bool ck = f32 && job->keep_state;
+    const int ckR = ck ? job->ck_ring_slots : 0;
+    const size_t o_ck32 = take(ck ? sizeof(int32_t) * 5 * n : 0);       // xp, rv, cell, sw, ckey
+    const size_t o_ck64 = take(ck ? sizeof(int64_t) * 2 * n : 0);       // cflip, nflip
+    const size_t o_ckr = take(ck ? sizeof(int64_t) * 2 * (size_t)ckR * n : 0);
     if (!alloc) return off;
     job->arena_bytes = off;
     // Stream-ordered allocation from the device pool: jobs created and freed
@@ -380,6 +386,14 @@ static size_t job_arena(ldp_job* job, bool alloc, void* at = nullptr) {
     job->d_means = (double*)(a + o_mean);
     job->d_ssum = f32 ? (int64_t*)(a + o_ssum) : nullptr;
     job->d_i32b = f32 ? (int32_t*)(a + o_i32b) : nullptr;
+    if (ck) {
+        int32_t* c32 = (int32_t*)(a + o_ck32);
+        job->ck_xp = (float*)c32; job->ck_rv = (float*)(c32 + n); job->ck_cell = c32 + 2 * n;
+        job->ck_sw = c32 + 3 * n; job->ck_ckey = c32 + 4 * n;
+        int64_t* c64 = (int64_t*)(a + o_ck64);
+        job->ck_cflip = c64; job->ck_nflip = c64 + n;
+        job->ck_ring = (void*)(a + o_ckr);
+    }
     if (nlag > 0 &&
         cudaMemcpyAsync(job->d_lags, job->lags.data(), sizeof(int64_t) * nlag, cudaMemcpyHostToDevice, st) !=
             cudaSuccess) {
@@ -475,8 +489,8 @@ extern "C" ldp_status ldp_job_set_precision(ldp_job* job, int precision) {
     if (!job) return LDP_ERR_INVALID;
     if (precision != LDP_PREC_FP64_PLAIN && precision != LDP_PREC_FP32_BATCHED) return LDP_ERR_INVALID;
     if (job->submitted || job->arena) return LDP_ERR_INVALID;
-    if (precision == LDP_PREC_FP32_BATCHED && (job->o.event_cap > 0 || job->p.number_of_previous_steps)) {
-        ldp_set_error(job->ctx, "per-event lists and restarts need the FP64 plain path");
+    if (precision == LDP_PREC_FP32_BATCHED && job->o.event_cap > 0) {
+        ldp_set_error(job->ctx, "per-event lists need the FP64 plain path");
         return LDP_ERR_UNSUPPORTED;
     }
     job->o.precision = precision;
@@ -508,7 +522,8 @@ static ldp_status submit_on(ldp_ctx* ctx, ldp_job* job, cudaStream_t s) {
         return LDP_ERR_NOMEM;
     }
     if (job->p.number_of_previous_steps && !job->restored) {
-        ldp_set_error(ctx, "NUMBEROFPREVIOUSSTEPS > 0 continues a restart: call ldp_job_restore first");
+        ldp_set_error(ctx, "NUMBEROFPREVIOUSSTEPS > 0 continues a run: call ldp_job_restore (FP64 plain) or "
+                           "ldp_job_load_state (FP32 batched) first");
         return LDP_ERR_INVALID;
     }
     job->submitted = true;
