@@ -421,8 +421,8 @@ ldp_status  ldp_job_write_outputs(ldp_job *job, const char *dir);
  * default stream) on the current device; the call returns without waiting.
  * Results equal ldp_job_create/ldp_submit with LDP_PREC_FP64_PLAIN for the
  * same params, layout and table_slots; RANDOMSEED < 0 means seed 0 here;
- * WAITINGTIME, WRITEX series and event lists (event_cap != 0) are not
- * produced, and FP32 precision or first-passage mode is rejected.  Errors
+ * WAITINGTIME, WRITEX series and event lists are not produced (event_cap
+ * > 0 is rejected; 0 and -1, automatic, mean none here), and FP32 precision or first-passage mode is rejected.  Errors
  * come back as a status and a message in err.
  */
 #define LDP_NOALLOC_MAX_TRAJ 4096

@@ -111,10 +111,10 @@ extern "C" ldp_status ldp_integrate_fp64_noalloc(const ldp_params* p, const ldp_
         set_err(err, errlen, m);
         return LDP_ERR_UNSUPPORTED;
     }
-    if (o->precision != LDP_PREC_FP64_PLAIN || o->mode != LDP_MODE_FIXED_STEPS || o->event_cap != 0 ||
+    if (o->precision != LDP_PREC_FP64_PLAIN || o->mode != LDP_MODE_FIXED_STEPS || o->event_cap > 0 ||
         p->waiting_time || p->n_cg > LDP_MAX_CG || p->freq_save < 1 || !(p->timestep > 0.0) ||
         !(p->periodic_length > 0.0) || p->number_of_previous_steps) {
-        set_err(err, errlen, "FP64 plain fixed-step runs only: no event lists (event_cap 0), WAITINGTIME off, at "
+        set_err(err, errlen, "FP64 plain fixed-step runs only: no event lists (event_cap <= 0), WAITINGTIME off, at "
                              "most 16 FPTCG entries, positive TIMESTEP and PERIODICLENGTH, FREQSAVE >= 1, no "
                              "restart (NUMBEROFPREVIOUSSTEPS 0)");
         return LDP_ERR_UNSUPPORTED;
