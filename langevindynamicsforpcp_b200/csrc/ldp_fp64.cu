@@ -279,14 +279,10 @@ struct FlipDraw {
 // z is the step's Gaussian; src supplies the flip schedule of a flip at s.
 // Returns 0 to continue, 1 when the trajectory stops before completing s
 // (non-finite position), 2 when it stops after s (first passage reached).
-template <bool DBL, bool OVER, bool ETA, class Src>
-__device__ __forceinline__ int fp64_step(const KConst& k, const TrajState& st, int64_t i, uint32_t g, T64& t,
-                                         uint64_t s, double z, const Src& src, int64_t& nflip, int64_t& sc0,
-                                         int64_t& sc1, uint32_t& flags, uint64_t& nxf) {
-    const int64_t n = st.n;
-    const uint64_t fs = k.freq_save;
-    const int64_t cell_prev = t.cell, well_prev = t.well;
-    const int lb_prev = t.lb;
+// The position (and velocity) update of a step, IntegrateStepEta's first
+// part (S.h:1680-1695, 2860-2870).
+template <bool OVER>
+__device__ __forceinline__ void fp64_move(const KConst& k, T64& t, double z) {
     if (OVER) {
         const double rf = k.sig_r * z;
         t.x = fma(t.F, k.c_drift, t.x);
@@ -299,6 +295,18 @@ __device__ __forceinline__ int fp64_step(const KConst& k, const TrajState& st, i
         t.v = k.expg * t.v + k.sig_v * z;
         t.x = t.x + t.v * k.hdt;
     }
+}
+
+// The rest of step s after fp64_move: indices, barrier flips and cell
+// entries, the state count, the force, the statistics and the frame.
+// cell_prev, well_prev, lb_prev: the indices before the move.
+template <bool DBL, bool OVER, bool ETA, class Src>
+__device__ __forceinline__ int fp64_after_move(const KConst& k, const TrajState& st, int64_t i, uint32_t g, T64& t,
+                                               uint64_t s, const Src& src, int64_t& nflip, int64_t& sc0,
+                                               int64_t& sc1, uint32_t& flags, uint64_t& nxf, int64_t cell_prev,
+                                               int64_t well_prev, int lb_prev) {
+    const int64_t n = st.n;
+    const uint64_t fs = k.freq_save;
     if (!isfinite(t.x)) {
         flags |= LDP_FLAG_NONFINITE;
         t.bits |= B_DONE;
@@ -465,6 +473,17 @@ __device__ __forceinline__ int fp64_step(const KConst& k, const TrajState& st, i
     return 0;
 }
 
+template <bool DBL, bool OVER, bool ETA, class Src>
+__device__ __forceinline__ int fp64_step(const KConst& k, const TrajState& st, int64_t i, uint32_t g, T64& t,
+                                         uint64_t s, double z, const Src& src, int64_t& nflip, int64_t& sc0,
+                                         int64_t& sc1, uint32_t& flags, uint64_t& nxf) {
+    const int64_t cell_prev = t.cell, well_prev = t.well;
+    const int lb_prev = t.lb;
+    fp64_move<OVER>(k, t, z);
+    return fp64_after_move<DBL, OVER, ETA>(k, st, i, g, t, s, src, nflip, sc0, sc1, flags, nxf, cell_prev, well_prev,
+                                           lb_prev);
+}
+
 // Steps s_begin .. s_end-1 of the hot loop, one trajectory per thread, each
 // drawing its own Gaussians (one Philox block per four steps) and flips.
 template <bool DBL, bool OVER, bool ETA>
@@ -576,6 +595,55 @@ struct FlipFromBuffer {
     }
 };
 
+// The open interval of positions (absolute x) in which a step cannot change
+// the cell, the well, the local barrier or the force: the interval between
+// the breakpoints of energy_force (and indices) around the current
+// cell-local position -- the cell edges, the barrier top 0, the flanks --
+// shrunk at both ends by a margin, 1e-9 (1 + |x|), far above the rounding of
+// x * invL and x - cell * L (~2e-16 |x|), so that for x inside it the full
+// step would compute the same indices and force.  Empty (lo > hi) when x is
+// within the margin of a breakpoint.
+template <bool DBL>
+__device__ __forceinline__ void quiet_band(const KConst& k, const T64& t, double* lo, double* hi) {
+    const double cL = (double)t.cell * k.L;
+    const double xp = t.x - cL;
+    const double hL = 0.5 * k.L;
+    double l = -hL, h = hL;
+    auto cut = [&](double b) {
+        if (b > -hL && b < hL) {
+            if (b <= xp) l = fmax(l, b);
+            if (b >= xp) h = fmin(h, b);
+        }
+    };
+    cut(0.0);
+    if (!DBL) {
+        cut(0.0 - k.w);
+        cut(k.w);
+    } else {
+        cut(k.lo0);
+        cut(k.xb[0]);
+        cut(k.xc);
+        cut(k.xb[1]);
+        cut(k.hi1);
+    }
+    const double m = 1e-9 * (1.0 + fabs(cL) + fabs(t.x));
+    *lo = cL + l + m;
+    *hi = cL + h - m;
+}
+
+// The force energy_force gives at the current position for either barrier
+// state (constant over the quiet band).
+template <bool DBL>
+__device__ __forceinline__ void band_forces(const KConst& k, const T64& t, double* f0, double* f1) {
+    T64 a = t;
+    a.state = 0;
+    energy_force<DBL>(k, a);
+    *f0 = a.F;
+    a.state = 1;
+    energy_force<DBL>(k, a);
+    *f1 = a.F;
+}
+
 __device__ __forceinline__ void named_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 __device__ __forceinline__ void named_arrive(int id) { asm volatile("bar.arrive %0, 64;" ::"r"(id) : "memory"); }
 
@@ -619,6 +687,9 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
     uint32_t flags = 0;
     uint64_t s = s_begin, nxf = 0;
     bool run = false, active = false;
+    // quiet band (empty: the first step takes the full path) and the force
+    // in it for either barrier state
+    double blo = 1.0, bhi = 0.0, bF0 = 0.0, bF1 = 0.0;
     if (lane == 0) {
         load_traj(st, t, i);
         active = run = !(t.bits & B_DONE);
@@ -635,11 +706,29 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
         if (lane == 0 && run) {
             const uint64_t s1 = (s_begin + (b + 1) * kLatBlock < s_end) ? s_begin + (b + 1) * kLatBlock : s_end;
             for (int l = 0; s < s1; ++s, ++l) {
+                const int64_t cell_prev = t.cell, well_prev = t.well;
+                const int lb_prev = t.lb;
+                fp64_move<OVER>(k, t, buf.z[u][l]);
+                if (t.x > blo && t.x < bhi && (int64_t)s != (int64_t)nxf) {
+                    // a quiet step: same indices, no frame, no event; a flip
+                    // toggles the state, takes its new schedule and the
+                    // band's force for that state (the rest of the full step)
+                    if (ETA && (int64_t)s == nflip) {
+                        t.state ^= 1;
+                        nflip = t.state ? buf.cand[u][1][l] : buf.cand[u][0][l];
+                        t.F = t.state ? bF1 : bF0;
+                    }
+                    if (t.state) ++sc1; else ++sc0;
+                    if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+                    continue;
+                }
                 const FlipFromBuffer src{&buf.cand[u][0][l], &buf.cand[u][1][l]};
-                const int r = fp64_step<DBL, OVER, ETA>(k, st, i, g, t, s, buf.z[u][l], src, nflip, sc0, sc1, flags,
-                                                        nxf);
+                const int r = fp64_after_move<DBL, OVER, ETA>(k, st, i, g, t, s, src, nflip, sc0, sc1, flags, nxf,
+                                                              cell_prev, well_prev, lb_prev);
                 if (r == 1) { run = false; break; }
                 if (r == 2) { ++s; run = false; break; }
+                quiet_band<DBL>(k, t, &blo, &bhi);
+                band_forces<DBL>(k, t, &bF0, &bF1);
             }
         }
         __syncwarp();
