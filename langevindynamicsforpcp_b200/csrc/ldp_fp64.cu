@@ -484,6 +484,55 @@ __device__ __forceinline__ int fp64_step(const KConst& k, const TrajState& st, i
                                            lb_prev);
 }
 
+// The open interval of positions (absolute x) in which a step cannot change
+// the cell, the well, the local barrier or the force: the interval between
+// the breakpoints of energy_force (and indices) around the current
+// cell-local position -- the cell edges, the barrier top 0, the flanks --
+// shrunk at both ends by a margin, 1e-9 (1 + |x|), far above the rounding of
+// x * invL and x - cell * L (~2e-16 |x|), so that for x inside it the full
+// step would compute the same indices and force.  Empty (lo > hi) when x is
+// within the margin of a breakpoint.
+template <bool DBL>
+__device__ __forceinline__ void quiet_band(const KConst& k, const T64& t, double* lo, double* hi) {
+    const double cL = (double)t.cell * k.L;
+    const double xp = t.x - cL;
+    const double hL = 0.5 * k.L;
+    double l = -hL, h = hL;
+    auto cut = [&](double b) {
+        if (b > -hL && b < hL) {
+            if (b <= xp) l = fmax(l, b);
+            if (b >= xp) h = fmin(h, b);
+        }
+    };
+    cut(0.0);
+    if (!DBL) {
+        cut(0.0 - k.w);
+        cut(k.w);
+    } else {
+        cut(k.lo0);
+        cut(k.xb[0]);
+        cut(k.xc);
+        cut(k.xb[1]);
+        cut(k.hi1);
+    }
+    const double m = 1e-9 * (1.0 + fabs(cL) + fabs(t.x));
+    *lo = cL + l + m;
+    *hi = cL + h - m;
+}
+
+// The force energy_force gives at the current position for either barrier
+// state (constant over the quiet band).
+template <bool DBL>
+__device__ __forceinline__ void band_forces(const KConst& k, const T64& t, double* f0, double* f1) {
+    T64 a = t;
+    a.state = 0;
+    energy_force<DBL>(k, a);
+    *f0 = a.F;
+    a.state = 1;
+    energy_force<DBL>(k, a);
+    *f1 = a.F;
+}
+
 // Steps s_begin .. s_end-1 of the hot loop, one trajectory per thread, each
 // drawing its own Gaussians (one Philox block per four steps) and flips.
 template <bool DBL, bool OVER, bool ETA>
@@ -511,6 +560,9 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
     double za = 0, zb = 0;
     uint32_t wc2 = 0, wc3 = 0;
     const FlipDraw src;
+    // quiet band (empty: the first step takes the full path) and the force
+    // in it for either barrier state
+    double blo = 1.0, bhi = 0.0, bF0 = 0.0, bF1 = 0.0;
     for (; s < s_end; ++s) {
         const int q = (int)((s - 1) & 3);
         if (q == 0 || s == s_begin) {
@@ -523,9 +575,29 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
             gauss_pair_f64(wc2, wc3, &za, &zb);
         }
         const double z = (q & 1) ? zb : za;
-        const int r = fp64_step<DBL, OVER, ETA>(k, st, i, g, t, s, z, src, nflip, sc0, sc1, flags, nxf);
+        const int64_t cell_prev = t.cell, well_prev = t.well;
+        const int lb_prev = t.lb;
+        fp64_move<OVER>(k, t, z);
+        if (t.x > blo && t.x < bhi && (int64_t)s != (int64_t)nxf) {
+            // a quiet step (see quiet_band): same indices, no frame, no
+            // event; a flip draws its schedule and takes the band's force
+            if (ETA && (int64_t)s == nflip) {
+                t.state ^= 1;
+                Words wf;
+                bool have = false;
+                nflip = src.schedule(k, g, s, t.state, &wf, &have);
+                t.F = t.state ? bF1 : bF0;
+            }
+            if (t.state) ++sc1; else ++sc0;
+            if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+            continue;
+        }
+        const int r = fp64_after_move<DBL, OVER, ETA>(k, st, i, g, t, s, src, nflip, sc0, sc1, flags, nxf, cell_prev,
+                                                      well_prev, lb_prev);
         if (r == 1) break;
         if (r == 2) { ++s; break; }
+        quiet_band<DBL>(k, t, &blo, &bhi);
+        band_forces<DBL>(k, t, &bF0, &bF1);
     }
     // s is the first step not integrated.
     st.counts[(int64_t)LDP_C_STATE0 * n + i] = sc0;
@@ -594,55 +666,6 @@ struct FlipFromBuffer {
         return state ? *c1 : *c0;
     }
 };
-
-// The open interval of positions (absolute x) in which a step cannot change
-// the cell, the well, the local barrier or the force: the interval between
-// the breakpoints of energy_force (and indices) around the current
-// cell-local position -- the cell edges, the barrier top 0, the flanks --
-// shrunk at both ends by a margin, 1e-9 (1 + |x|), far above the rounding of
-// x * invL and x - cell * L (~2e-16 |x|), so that for x inside it the full
-// step would compute the same indices and force.  Empty (lo > hi) when x is
-// within the margin of a breakpoint.
-template <bool DBL>
-__device__ __forceinline__ void quiet_band(const KConst& k, const T64& t, double* lo, double* hi) {
-    const double cL = (double)t.cell * k.L;
-    const double xp = t.x - cL;
-    const double hL = 0.5 * k.L;
-    double l = -hL, h = hL;
-    auto cut = [&](double b) {
-        if (b > -hL && b < hL) {
-            if (b <= xp) l = fmax(l, b);
-            if (b >= xp) h = fmin(h, b);
-        }
-    };
-    cut(0.0);
-    if (!DBL) {
-        cut(0.0 - k.w);
-        cut(k.w);
-    } else {
-        cut(k.lo0);
-        cut(k.xb[0]);
-        cut(k.xc);
-        cut(k.xb[1]);
-        cut(k.hi1);
-    }
-    const double m = 1e-9 * (1.0 + fabs(cL) + fabs(t.x));
-    *lo = cL + l + m;
-    *hi = cL + h - m;
-}
-
-// The force energy_force gives at the current position for either barrier
-// state (constant over the quiet band).
-template <bool DBL>
-__device__ __forceinline__ void band_forces(const KConst& k, const T64& t, double* f0, double* f1) {
-    T64 a = t;
-    a.state = 0;
-    energy_force<DBL>(k, a);
-    *f0 = a.F;
-    a.state = 1;
-    energy_force<DBL>(k, a);
-    *f1 = a.F;
-}
 
 __device__ __forceinline__ void named_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 __device__ __forceinline__ void named_arrive(int id) { asm volatile("bar.arrive %0, 64;" ::"r"(id) : "memory"); }
