@@ -67,11 +67,12 @@ def test_chain_of_three_with_small_launches(tmp_path):
     from langevindynamicsforpcp_b200 import _tune
     with ldp.Context(0) as c:
         _tune.set_fp32_shape(c, block=128, blocks_per_sm=1, pair_budget=1500)
-        whole = run(c, params("single_over", 36_000), lanes=30_000)
+        f = {"freq_save": 10}        # 1200 frames per link (at least 1000)
+        whole = run(c, params("single_over", 36_000, **f), lanes=30_000)
         a, b = str(tmp_path / "a.state"), str(tmp_path / "b.state")
-        run(c, params("single_over", 12_000), state_out=a, lanes=30_000)
-        run(c, params("single_over", 12_000, prev=12_000), state_in=a, state_out=b, lanes=30_000)
-        cont = run(c, params("single_over", 12_000, prev=24_000), state_in=b, lanes=30_000)
+        run(c, params("single_over", 12_000, **f), state_out=a, lanes=30_000)
+        run(c, params("single_over", 12_000, prev=12_000, **f), state_in=a, state_out=b, lanes=30_000)
+        cont = run(c, params("single_over", 12_000, prev=24_000, **f), state_in=b, lanes=30_000)
     for k in ("counts", "sums", "x_final", "v_final", "state_final", "frames_x", "msd"):
         np.testing.assert_array_equal(cont[k], whole[k], err_msg=k)
 
