@@ -339,7 +339,8 @@ typedef struct ldp_server_opts {
     int64_t hbm_budget;     /* bytes of job arenas resident at once (0: 80% of free memory,
                                counting what the device's memory pool holds unused)        */
     int64_t pair_budget;    /* step pairs per slot per persistent launch (0: 1024)           */
-    int32_t max_inflight;   /* persistent launches in flight per model type (1..16)         */
+    int32_t max_inflight;   /* persistent launches in flight (1..16; each covers every
+                               model type's queue)                                          */
     int32_t region;         /* 1 (default): allocate the budget once, at creation, as one
                                device region that admitted jobs' arenas are placed in (no
                                device allocation per job); 0: each arena from the device's
@@ -361,6 +362,11 @@ ldp_status  ldp_server_submit(ldp_server *s, const ldp_params *p, const ldp_job_
 ldp_status  ldp_server_step(ldp_server *s, int *ndone);
 /* state: ldp_server_state; latency_s: submission to done (0 until done). */
 ldp_status  ldp_server_poll(ldp_server *s, uint64_t ticket, int *state, double *latency_s);
+/* Tickets of jobs that ended (done or failed) since the last call, oldest
+ * first: up to cap of them into tickets, *n = how many; with cap 0, *n = how
+ * many are waiting (none taken).  A host loop driving many jobs polls only
+ * these instead of every ticket. */
+ldp_status  ldp_server_take_ended(ldp_server *s, uint64_t *tickets, int64_t cap, int64_t *n);
 /* Seconds from submission to admission, to all trajectories retired, and to
  * done (-1 for a stage not reached yet): where a job's latency went. */
 ldp_status  ldp_server_job_times(ldp_server *s, uint64_t ticket, double times[3]);

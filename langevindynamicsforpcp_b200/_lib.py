@@ -162,6 +162,7 @@ SIGNATURES = {
     "ldp_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "ldp_server_job": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p)]),
     "ldp_server_job_times": (C.c_int, [C.c_void_p, C.c_uint64, _DP]),
+    "ldp_server_take_ended": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int64, C.POINTER(C.c_int64)]),
     "ldp_server_release": (C.c_int, [C.c_void_p, C.c_uint64]),
     "ldp_server_info_get": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
     "ldp_server_destroy": (None, [C.c_void_p]),

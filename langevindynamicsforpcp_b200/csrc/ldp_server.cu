@@ -85,6 +85,7 @@ struct ldp_server {
     std::vector<Entry*> running;         // integrating
     std::vector<Entry*> finishing;       // post-processing enqueued
     std::unordered_map<uint64_t, Entry*> all;
+    std::deque<uint64_t> ended;          // tickets done or failed, not yet taken
     uint64_t next_ticket = 1;
     unsigned long long* h_rem[4] = {};   // pinned copies of the queues' counters
     cudaEvent_t rem_ev[4] = {};
@@ -282,6 +283,10 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
             if (idle) {
                 en->state = LDP_SRV_FAILED;
                 en->t_done = now_s();
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    s->ended.push_back(en->ticket);
+                }
                 ldp_set_error(ctx, "job %llu: device allocation of %zu bytes failed",
                               (unsigned long long)en->ticket, en->bytes);
                 continue;
@@ -426,6 +431,10 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
         job->done = true;
         en->state = LDP_SRV_DONE;
         en->t_done = now_s();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->ended.push_back(en->ticket);
+        }
         ++done;
         s->finishing[i] = s->finishing.back();
         s->finishing.pop_back();
@@ -445,6 +454,22 @@ extern "C" ldp_status ldp_server_poll(ldp_server* s, uint64_t ticket, int* state
     *state = en->state;
     if (latency_s) *latency_s = (en->state == LDP_SRV_DONE || en->state == LDP_SRV_FAILED) ? en->t_done - en->t_submit
                                                                                           : 0.0;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_server_take_ended(ldp_server* s, uint64_t* tickets, int64_t cap, int64_t* n) {
+    if (!s || !n || cap < 0 || (cap > 0 && !tickets)) return LDP_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (cap == 0) {
+        *n = (int64_t)s->ended.size();
+        return LDP_OK;
+    }
+    int64_t k = 0;
+    while (k < cap && !s->ended.empty()) {
+        tickets[k++] = s->ended.front();
+        s->ended.pop_front();
+    }
+    *n = k;
     return LDP_OK;
 }
 

@@ -103,6 +103,17 @@ class Server:
         _check(L.lib().ldp_server_poll(self.handle, ticket, C.byref(st), C.byref(lat)), self.ctx)
         return st.value, lat.value
 
+    def ended(self, cap: int = 4096) -> list:
+        """Tickets of the jobs that ended (done or failed) since the last call."""
+        buf = (C.c_uint64 * cap)()
+        n = C.c_int64(0)
+        out = []
+        while True:
+            _check(L.lib().ldp_server_take_ended(self.handle, buf, cap, C.byref(n)), self.ctx)
+            out.extend(buf[:n.value])
+            if n.value < cap:
+                return out
+
     def times(self, ticket: int):
         """(admitted, trajectories retired, done), seconds after submission."""
         t = (C.c_double * 3)()
@@ -177,26 +188,27 @@ def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 
             p, ntraj, _ = work[nxt]
             tickets[server.submit(p, ntraj, job_id=nxt)] = nxt
             nxt += 1
-        if server.step() or True:
-            for t in list(tickets):
-                st, l = server.poll(t)
-                if st == L.SRV_DONE or st == L.SRV_FAILED:
-                    i = tickets.pop(t)
-                    if st == L.SRV_FAILED:
-                        raise RuntimeError(f"job {i} failed: {server.ctx.last_error()}")
-                    lat[i] = l
-                    if stages is not None:
-                        stages[i] = server.times(t)
-                    if on_done:
-                        on_done(i, server.job(t))
-                    server.release(t)
+        server.step()
+        for t in server.ended():
+            if t not in tickets:
+                continue
+            st, l = server.poll(t)
+            i = tickets.pop(t)
+            if st == L.SRV_FAILED:
+                raise RuntimeError(f"job {i} failed: {server.ctx.last_error()}")
+            lat[i] = l
+            if stages is not None:
+                stages[i] = server.times(t)
+            if on_done:
+                on_done(i, server.job(t))
+            server.release(t)
         if not tickets and nxt < n:
             time.sleep(max(0.0, min(arrivals[nxt] - (time.perf_counter() - t0), 0.01)))
     return lat
 
 
 def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: int = 24000, loads=(0.5, 0.8),
-            isolated_sample: int = 24, device: int = 0) -> dict:
+            isolated_sample: int = 24, device: int = 0, pair_budget: int = 1024, max_inflight: int = 2) -> dict:
     """Capacity (every job submitted at once), isolated solve times and, per
     offered load (a fraction of that capacity), the latency distribution of
     a Poisson stream of the serving workload's jobs."""
@@ -206,16 +218,22 @@ def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: in
     psteps = float(sum(n for _, n, _ in work)) * a.steps
     out = {"workload": f"serving: {a.jobs} jobs, types single/double x over/underdamped, "
                        f"2^U[{a.exp_lo:g},{a.exp_hi:g}] trajectories, {a.steps} steps", "loads": {}}
-    with Context(device) as ctx, Server(ctx) as srv:
+    out["launch"] = {"pair_budget": pair_budget, "max_inflight": max_inflight}
+    with Context(device) as ctx, Server(ctx, pair_budget=pair_budget, max_inflight=max_inflight) as srv:
         # warm-up (first launches of each kernel, first use of each queue)
         run_stream(srv, serving_workload(32, seed=99, exp_lo=a.exp_lo, exp_hi=a.exp_hi, steps=a.steps),
                    np.zeros(32))
         # capacity: every job submitted at once
+        i0 = srv.info()
         t = time.perf_counter()
         run_stream(srv, work, np.zeros(len(work)))
         makespan = time.perf_counter() - t
         cap = len(work) / makespan
         out["capacity"] = {"jobs_per_s": cap, "particle_steps_per_s": psteps / makespan, "makespan_s": makespan}
+        i1 = srv.info()
+        out["capacity"]["host_loop"] = {
+            "steps": i1["steps"] - i0["steps"], "launches": i1["launches"] - i0["launches"],
+            "phase_s": [b - a for a, b in zip(i0["phase_s"], i1["phase_s"])], "phase_max_s": i1["phase_max_s"]}
         # isolated solve time: each job alone in the server (every job when
         # --isolated-sample covers them all, else a sample interpolated by
         # trajectory count within the job's model type)
@@ -280,8 +298,11 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=24000)
     ap.add_argument("--loads", type=float, nargs="+", default=[0.5, 0.8])
     ap.add_argument("--isolated-sample", type=int, default=24)
+    ap.add_argument("--pair-budget", type=int, default=1024, help="step pairs per slot per persistent launch")
+    ap.add_argument("--max-inflight", type=int, default=2, help="persistent launches in flight")
     a = ap.parse_args(argv)
-    print(json.dumps(measure(a.jobs, a.exp_lo, a.exp_hi, a.steps, a.loads, a.isolated_sample)))
+    print(json.dumps(measure(a.jobs, a.exp_lo, a.exp_hi, a.steps, a.loads, a.isolated_sample,
+                             pair_budget=a.pair_budget, max_inflight=a.max_inflight)))
 
 
 if __name__ == "__main__":

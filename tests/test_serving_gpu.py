@@ -60,13 +60,17 @@ def test_admission_respects_the_memory_budget():
                 info = srv.info()
                 peak = max(peak, info["hbm_in_use"])
                 assert info["hbm_in_use"] <= budget
-                for t in tickets:
+                ended = srv.ended()
+                for t in tickets:   # the ended list names exactly the jobs that became done
                     if t not in done and srv.poll(t)[0] == L.SRV_DONE:
+                        assert t in ended
                         done.add(t)
                         srv.release(t)
+                assert set(ended) <= done
                 if len(done) == len(tickets):
                     break
             assert len(done) == len(tickets)
+            assert srv.ended() == []
             assert peak >= min(sizes)
             # Arenas live in the server's region: released jobs give their
             # space back and freed neighbours merge, so a job of about twice
