@@ -246,12 +246,14 @@ def compare_summaries(a, b):
     return out
 
 
-def quick_test_leg(ldp, ctx, job_id0):
+def quick_test_leg(ldp, ctx, job_id0, nsteps=None):
     """The reference's sample (C1) through the FP64 plain path: ns per step
     of its 32 trajectories and the projected wall time of the full 3e9-step
-    run, beside the reference's recorded time."""
+    run, beside the reference's recorded time (nsteps: a shorter run, for
+    profiling)."""
+    steps = nsteps or QT_STEPS
     p = ldp.params_from_inp(os.path.join(ROOT, "tests", "golden", "inp", "quick_test__2.0_7.2_m1.0_1.00e-05.inp"))
-    p.number_of_steps, p.freq_save, p.random_seed = QT_STEPS, QT_STEPS // 2000, 1234
+    p.number_of_steps, p.freq_save, p.random_seed = steps, steps // 2000, 1234
     p.write_restart = 0
     with ldp.Job(ctx, p, lanes=8, ranks=4, job_id=job_id0) as j:
         ctx.mark(4)
@@ -259,10 +261,10 @@ def quick_test_leg(ldp, ctx, job_id0):
         j.wait()
         ctx.mark(5)
         ms = ctx.elapsed_ms(4, 5)
-    ns_step = ms * 1e6 / QT_STEPS
+    ns_step = ms * 1e6 / steps
     return {"workload": "sample_input/quick_test .inp verbatim, 4 ranks x 8 lanes = 32 trajectories, "
-                        f"{QT_STEPS} steps (FREQSAVE {QT_STEPS // 2000})",
-            "ms": ms, "ns_per_step": ns_step, "particle_steps_per_s": 32 * QT_STEPS / (ms * 1e-3),
+                        f"{steps} steps (FREQSAVE {steps // 2000})",
+            "ms": ms, "ns_per_step": ns_step, "particle_steps_per_s": 32 * steps / (ms * 1e-3),
             "projected_full_run_s": ns_step * 1e-9 * QT_FULL_STEPS,
             "reference_full_run_s": QT_REF_S,
             "reference_note": "16 trajectories x 3e9 steps on 4 Xeon Gold 6136 ranks (executed_job time.log)"}
@@ -357,6 +359,8 @@ def main():
     ap.add_argument("--njobs", type=int, default=None, help="jobs per batch (profiling cases)")
     ap.add_argument("--freqsave", type=int, default=None, help="steps between frames (profiling cases)")
     ap.add_argument("--ntraj", type=int, default=None, help="trajectories per job (profiling cases)")
+    ap.add_argument("--leg", default="all", choices=["all", "fp32", "fp64", "quick_test"],
+                    help="profiling cases: run one leg and print its timing only (not a bench line)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -396,13 +400,19 @@ def main():
         rep.barrier()
         torch.cuda.synchronize()
 
+    if args.leg == "quick_test":
+        print(json.dumps({"leg": "quick_test", **quick_test_leg(ldp, ctx, job_id0, args.nsteps)}), flush=True)
+        ctx.close()
+        rep.close()
+        return
+
     # ---- FP32 batched, device-resident timing ----
-    for _ in range(args.warmup):
+    for _ in range(args.warmup if args.leg in ("all", "fp32") else 0):
         for j in run_batch(ldp, ctx, params, ldp.PREC_FP32_BATCHED, job_id0):
             j.close()
     times, kernel_ms, msd_ms, launches = [], [], [], 0
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(args.steps if args.leg in ("all", "fp32") else 0):
             jobs = [ldp.Job(ctx, p, lanes=NTRAJ, precision=ldp.PREC_FP32_BATCHED, job_id=job_id0 + i)
                     for i, p in enumerate(params)]
             flush_l2()
@@ -423,7 +433,14 @@ def main():
             for j in jobs:
                 j.close()
     clocks = clk.summary()
-    step_ms = rep.max_over_ranks(sum(times) / len(times))
+    if args.leg == "fp32":
+        print(json.dumps({"leg": "fp32", "ms_per_step": sum(times) / len(times),
+                          "kernel_ms": sum(kernel_ms) / len(kernel_ms),
+                          "particle_steps_per_s": psteps / (sum(times) / len(times) * 1e-3)}), flush=True)
+        ctx.close()
+        rep.close()
+        return
+    step_ms = rep.max_over_ranks(sum(times) / len(times)) if times else float("nan")
     value = psteps * world / (step_ms * 1e-3)
     shape_used = _tune.get_fp32_shape(ctx)
 
@@ -431,7 +448,7 @@ def main():
     # (the batch runs the FP64 jobs side by side on two streams); one
     # untimed pass, then FP64_STEPS timed passes.
     t64 = []
-    for it in range(1 + FP64_STEPS):
+    for it in range(1 + (FP64_STEPS if args.leg == "all" else args.steps)):
         jobs64 = [ldp.Job(ctx, p, lanes=NTRAJ, precision=ldp.PREC_FP64_PLAIN, job_id=job_id0 + i)
                   for i, p in enumerate(params)]
         flush_l2()
@@ -447,6 +464,11 @@ def main():
             j.close()
     fp64_ms = rep.max_over_ranks(sum(t64) / len(t64))
     fp64_value = psteps / (fp64_ms * 1e-3)
+    if args.leg == "fp64":
+        print(json.dumps({"leg": "fp64", "ms_per_step": fp64_ms, "particle_steps_per_s": fp64_value}), flush=True)
+        ctx.close()
+        rep.close()
+        return
     accuracy = accuracy_leg(ldp, ctx, job_id0)
     quick_test = quick_test_leg(ldp, ctx, job_id0)
     serving = serving_leg(local) if not args.no_serving else None

@@ -208,7 +208,8 @@ def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 
 
 
 def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: int = 24000, loads=(0.5, 0.8),
-            isolated_sample: int = 24, device: int = 0, pair_budget: int = 1024, max_inflight: int = 2) -> dict:
+            isolated_sample: int = 24, device: int = 0, pair_budget: int = 1024, max_inflight: int = 2,
+            hbm_budget: int = 0) -> dict:
     """Capacity (every job submitted at once), isolated solve times and, per
     offered load (a fraction of that capacity), the latency distribution of
     a Poisson stream of the serving workload's jobs."""
@@ -219,7 +220,8 @@ def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: in
     out = {"workload": f"serving: {a.jobs} jobs, types single/double x over/underdamped, "
                        f"2^U[{a.exp_lo:g},{a.exp_hi:g}] trajectories, {a.steps} steps", "loads": {}}
     out["launch"] = {"pair_budget": pair_budget, "max_inflight": max_inflight}
-    with Context(device) as ctx, Server(ctx, pair_budget=pair_budget, max_inflight=max_inflight) as srv:
+    with Context(device) as ctx, Server(ctx, hbm_budget=hbm_budget, pair_budget=pair_budget,
+                                        max_inflight=max_inflight) as srv:
         # warm-up (first launches of each kernel, first use of each queue)
         run_stream(srv, serving_workload(32, seed=99, exp_lo=a.exp_lo, exp_hi=a.exp_hi, steps=a.steps),
                    np.zeros(32))
@@ -296,13 +298,15 @@ def main(argv=None):
     ap.add_argument("--exp-lo", type=float, default=10)
     ap.add_argument("--exp-hi", type=float, default=18)
     ap.add_argument("--steps", type=int, default=24000)
-    ap.add_argument("--loads", type=float, nargs="+", default=[0.5, 0.8])
+    ap.add_argument("--loads", type=float, nargs="*", default=[0.5, 0.8])
     ap.add_argument("--isolated-sample", type=int, default=24)
     ap.add_argument("--pair-budget", type=int, default=1024, help="step pairs per slot per persistent launch")
     ap.add_argument("--max-inflight", type=int, default=2, help="persistent launches in flight")
+    ap.add_argument("--hbm-budget", type=float, default=0, help="GB of job arenas resident at once (0: 80 %% of free)")
     a = ap.parse_args(argv)
     print(json.dumps(measure(a.jobs, a.exp_lo, a.exp_hi, a.steps, a.loads, a.isolated_sample,
-                             pair_budget=a.pair_budget, max_inflight=a.max_inflight)))
+                             pair_budget=a.pair_budget, max_inflight=a.max_inflight,
+                             hbm_budget=int(a.hbm_budget * 1e9))))
 
 
 if __name__ == "__main__":
