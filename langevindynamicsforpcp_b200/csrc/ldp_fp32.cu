@@ -1025,9 +1025,13 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_persistent_kern
 // All four model types in one persistent launch (the serving loop's).  A
 // warp serves one type at a time -- a warp-uniform switch over the four
 // instantiated loops -- with every lane's trajectory from that type's queue;
-// when all its lanes are idle and that queue is dry it takes the next type
-// with unclaimed items (round robin from a start spread over warps), so no
-// type's work waits for another type's launch.  The warp's type is kept
+// when all its lanes are idle and that queue is dry it takes another type
+// with unclaimed items, so no type's work waits for another type's launch.
+// Its pick is the type its SM serves (sm_type) while that queue has work,
+// else the first type with work round robin from the SM's index, which then
+// becomes the SM's type: the warps of an SM converge on one type, whose code
+// alone then fills the SM's instruction caches (warps of different types on
+// one SM measured as stalls on instruction fetch).  The warp's type is kept
 // across launches in wtype (-1: none).  A warp ends its launch when the
 // budget is spent, no queue has work, or eight type changes in a row found
 // nothing to claim (claims raced away by other warps).
@@ -1043,15 +1047,26 @@ __global__ void __launch_bounds__(256, LDP_FP32_MIN_BLOCKS) fp32_mixed_kernel(co
         if (type < 0) {
             int pick = -1;
             if ((threadIdx.x & 31) == 0) {
-                const int start = (int)(w & 3);
-                for (int k = 0; k < 4; ++k) {
-                    const int tt = (start + k) & 3;
+                unsigned smid;
+                asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+                volatile int32_t* home = m.sm_type + (smid & (unsigned)(kMixedSmTypes - 1));
+                auto has_work = [&](int tt) {
                     const unsigned long long h = *(volatile const unsigned long long*)m.q[tt].head;
                     const unsigned long long tl = *(volatile const unsigned long long*)m.q[tt].tail;
-                    if (h < tl) {
-                        pick = tt;
-                        break;
+                    return h < tl;
+                };
+                const int pref = *home;
+                if (pref >= 0 && pref < 4 && has_work(pref)) {
+                    pick = pref;
+                } else {
+                    for (int k = 0; k < 4; ++k) {
+                        const int tt = (int)((smid + (unsigned)k) & 3u);
+                        if (has_work(tt)) {
+                            pick = tt;
+                            break;
+                        }
                     }
+                    if (pick >= 0) *home = pick;
                 }
             }
             pick = __shfl_sync(kFull, pick, 0);

@@ -121,11 +121,15 @@ struct SlotsDev {
 
 // The four model types' queues and one set of slots shared by them, for the
 // mixed persistent kernel (the serving loop's launches); wtype[w] is the
-// type warp w serves (-1: none).
+// type warp w serves (-1: none); sm_type[smid & (kMixedSmTypes - 1)] the type
+// the warps of an SM take first when they pick one (-1: none), so that an SM
+// runs one type's code at a time.
+constexpr int kMixedSmTypes = 1024;
 struct MixedDev {
     QueueDev q[4];
     SlotsDev S;
     int32_t* wtype;
+    int32_t* sm_type;
     int64_t nwarps;
 };
 

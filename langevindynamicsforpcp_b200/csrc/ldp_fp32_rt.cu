@@ -283,14 +283,16 @@ int fp32_launch_mixed(ldp_ctx* ctx, uint32_t pair_budget, cudaStream_t st) {
         const int64_t nslots = (int64_t)R.mixed_grid * block;
         int e = slots_init(nslots, ring, &R.mixed, &R.mixed_mem);
         if (e) return e;
-        cudaError_t ce = cudaMalloc((void**)&R.wtype, sizeof(int32_t) * (size_t)(nslots / 32));
-        if (ce == cudaSuccess) ce = cudaMemset(R.wtype, 0xff, sizeof(int32_t) * (size_t)(nslots / 32));   // -1
+        const size_t n = (size_t)(nslots / 32) + kMixedSmTypes;   // wtype, then sm_type
+        cudaError_t ce = cudaMalloc((void**)&R.wtype, sizeof(int32_t) * n);
+        if (ce == cudaSuccess) ce = cudaMemset(R.wtype, 0xff, sizeof(int32_t) * n);   // -1
         if (ce != cudaSuccess) return (int)ce;
     }
     MixedDev m;
     for (int t = 0; t < 4; ++t) m.q[t] = R.q[t].q;
     m.S = R.mixed;
     m.wtype = R.wtype;
+    m.sm_type = R.wtype + R.mixed.nslots / 32;
     m.nwarps = R.mixed.nslots / 32;
     return launch_fp32_mixed(m, pair_budget, R.mixed_grid, 256, st);
 }
