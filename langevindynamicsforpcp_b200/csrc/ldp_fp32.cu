@@ -71,6 +71,9 @@ struct RareSm {
     // the lane state only the general step uses.
     float xp[kMaxBlock], rv[kMaxBlock], F[kMaxBlock], lo[kMaxBlock], hi[kMaxBlock], c1[kMaxBlock];
     uint32_t traj[kMaxBlock];
+    uint32_t gtraj[kMaxBlock];    // the trajectory's random-stream index (traj + the job's g0)
+    uint32_t key0[kMaxBlock], key1[kMaxBlock];
+    float kn[kMaxBlock];
     long long nflip[kMaxBlock];   // step of the current barrier's next flip
     int32_t left[kMaxBlock], job[kMaxBlock], cell[kMaxBlock], state[kMaxBlock], sw[kMaxBlock];
 };
@@ -406,6 +409,19 @@ __device__ __noinline__ void f_keep_state(const JobF* Jp, const SlotsDev* Sp, co
     J.tpt2_last[traj] = sm.tpt2[t];
 }
 
+// Ends a lane's trajectory after step `done` (general step): keeps its
+// continuation state when the job asks for it and the trajectory completed,
+// then retires it.  The lane's cell, state and slot word in sm are current.
+template <bool OVER>
+__device__ __noinline__ void f_end_lane(const JobF* Jp, const SlotsDev* Sp, RareSm* smp, int t, int64_t slot,
+                                        uint64_t done, float xp, float v, float rv, uint32_t flags) {
+    const JobF& J = *Jp;
+    RareSm& sm = *smp;
+    if (J.ck_xp && !flags && done == J.nsteps)
+        f_keep_state(Jp, Sp, smp, t, slot, sm.traj[t], xp, OVER ? rv : v, sm.cell[t], sm.sw[t]);
+    retire_lane<OVER>(J, Sp->retired, sm, t, done, xp, v, flags);
+}
+
 // The general step s of one lane (position already advanced):
 // the FP64 step order of ldp_fp64.cu from the index update on.  Out of line,
 // on the lane state in shared memory, so that the hot loop's registers do
@@ -430,8 +446,8 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
     auto retire = [&](uint64_t done, float v, uint32_t flags) {
         sm.cell[t] = cell;
         sm.state[t] = state;
-        if (J.ck_xp && !flags && done == J.nsteps) f_keep_state(&J, &S, &sm, t, slot, traj, xp, OVER ? rv : v, cell, sw);
-        retire_lane<OVER>(J, S.retired, sm, t, done, xp, v, flags);
+        sm.sw[t] = sw;
+        f_end_lane<OVER>(&J, &S, &sm, t, slot, done, xp, v, rv, flags);
         sm.job[t] = -1;
         sm.lo[t] = -kInf;
         sm.hi[t] = kInf;
@@ -595,6 +611,23 @@ __device__ __noinline__ void general_step(const JobF* jobs, const SlotsDev* Sp, 
         return done;
     };
 
+    if (J.eta && xp > lo && xp < hi && (long long)s == sm.nflip[t] && (long long)s != sm.nxf[t] &&
+        s != J.nsteps && (xp < 0.0f) == (lo < 0.0f) && (!DBL || (xp < J.xc ? 0 : W_LB) == (sw & W_LB))) {
+        // Only the current barrier's flip (no band exit, so the same cell,
+        // well and local barrier; no frame; not the last step): the path
+        // below with flip alone -- the new state and its schedule, the
+        // state-1 run, the state's force, the countdown.
+        const int st = state ^ 1;
+        const Words w = philox_at(s, gp, TAG_FLIP, J.key0, J.key1);
+        const long long nf = flip_schedule(s, w.w0, w.w1, J.ln1m[st]);
+        if (st) sm.since[t] = (long long)s;
+        else sm.sc1[t] += (long long)s - sm.since[t];
+        sm.state[t] = st;
+        sm.nflip[t] = nf;
+        sm.F[t] = force_of<DBL>(J, xp, st);
+        sm.left[t] = steps_to_special(J, s, sm.nxf[t], nf);
+        return;
+    }
     if (xp > lo && xp < hi && (long long)s != sm.nflip[t]) {
         // Only the countdown ran out: a frame and/or the last step.
         const float F = sm.F[t];
@@ -814,14 +847,10 @@ __device__ __forceinline__ uint32_t persistent_run(const QueueDev& q, const Slot
 
     // ---- hot lane state (registers); the rest lives in sm ----
     int job = (slot < S.nslots) ? S.job[slot] : -1;
-    // the lane's trajectory: job-local index in sm.traj, its random-stream
-    // index (plus the job's g0) in a register
-    uint32_t ptraj = 0;
     uint64_t j = 0;                 // next block of four steps: 4j+1 .. 4j+4
     float xp = 0.f, rv = 0.f, F = 0.f, lo = -kInf, hi = kInf;
     int left = kLeftMax;
-    float c1 = 0.f, c2 = 0.f, c3 = 0.f, kn = 0.f;
-    uint32_t key0 = 0, key1 = 0;
+    float c1 = 0.f, c2 = 0.f, c3 = 0.f;
     sm.job[t] = job;
 
     // Per-job constants into registers; band, force and countdown from the
@@ -832,10 +861,10 @@ __device__ __forceinline__ uint32_t persistent_run(const QueueDev& q, const Slot
         else { c1 = J.hdt_invM; c2 = J.hdt; c3 = J.expg; }
         sm.c1[t] = c1;
         sm.traj[t] = traj;
-        kn = J.bm_k;
-        key0 = J.key0;
-        key1 = J.key1;
-        ptraj = traj + J.g0;
+        sm.kn[t] = J.bm_k;
+        sm.key0[t] = J.key0;
+        sm.key1[t] = J.key1;
+        sm.gtraj[t] = traj + J.g0;
         const int state = sm.state[t];
         band_of<DBL>(J, xp, &lo, &hi);
         F = force_of<DBL>(J, xp, state);
@@ -934,7 +963,8 @@ __device__ __forceinline__ uint32_t persistent_run(const QueueDev& q, const Slot
         }
 
         // ---- one Philox block, four steps ----
-        const Words w = philox_wide((uint32_t)j, (uint32_t)(j >> 32), ptraj, TAG_STEP, key0, key1);
+        const Words w = philox_wide((uint32_t)j, (uint32_t)(j >> 32), sm.gtraj[t], TAG_STEP, sm.key0[t], sm.key1[t]);
+        const float kn = sm.kn[t];
         float nq[4];
         noise_pair(w.w0, w.w1, kn, &nq[0], &nq[1]);
         noise_pair(w.w2, w.w3, kn, &nq[2], &nq[3]);
