@@ -273,7 +273,8 @@ def quick_test_leg(ldp, ctx, job_id0, nsteps=None):
 # Serving leg: SERVE_JOBS jobs of the serving workload (types single/double x
 # over/underdamped, 2^U[10,18] trajectories, 24000 steps, parameters from the
 # precision / batching / scan ranges): capacity with every job submitted at
-# once, then Poisson streams at 50 % and 80 % of it.  The full workload is
+# once, the capacity sustained under Poisson arrivals offered at that rate,
+# then Poisson streams at 50 % and 80 % of the smaller.  The full workload is
 # 10^4 jobs (langevindynamicsforpcp_b200.serve); this many fit the bench.
 SERVE_JOBS = 1000
 
@@ -282,12 +283,13 @@ def serving_leg(device):
     """p50 / p99 job latency of the serving loop (its own context)."""
     from langevindynamicsforpcp_b200 import serve
     r = serve.measure(jobs=SERVE_JOBS, loads=(0.5, 0.8), isolated_sample=24, device=device)
-    out = {"workload": r["workload"], "capacity": r["capacity"], "isolated": r["isolated"], "loads": {}}
+    out = {"workload": r["workload"], "capacity": r["capacity"], "sustained": r["sustained"],
+           "isolated": r["isolated"], "loads": {}}
     for load, v in r["loads"].items():
         out["loads"][load] = {k: v[k] for k in ("rate_jobs_per_s", "p50_latency_s", "p99_latency_s",
                                                 "p50_over_isolated", "p99_over_isolated",
                                                 "p99_latency_over_p99_isolated", "particle_steps_per_s",
-                                                "by_trajectory_count")}
+                                                "by_trajectory_count", "p99_stage_s")}
     return out
 
 

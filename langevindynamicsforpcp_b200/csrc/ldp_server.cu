@@ -9,11 +9,12 @@
 //     (allocated once: no device allocation per job, which can stall the
 //     loop for seconds while the pool grows) and registering them with the
 //     work queue of their model type;
-//  2. publishes admitted jobs' trajectories to the queue in chunks, keeping
-//     about half a wave of slots' worth of unclaimed work queued and always
-//     publishing next for the job with the fewest unpublished trajectories
-//     (shortest remaining first): a small job that arrives while large ones
-//     run starts within one chunk, instead of after every earlier job;
+//  2. publishes admitted jobs' trajectories to their type's queue in chunks,
+//     keeping about as much unclaimed work queued as the launches in flight
+//     and the next one will claim, and always publishing next for the job
+//     with the fewest unpublished trajectories of any type (shortest
+//     remaining first): a small job that arrives while large ones run
+//     starts within about one launch, instead of after every earlier job;
 //  3. keeps up to `max_inflight` short persistent launches (pair budget
 //     `pair_budget`) in flight while any job is active, each over all four
 //     model types' queues (a warp serves one type at a time and moves to
@@ -320,28 +321,42 @@ extern "C" ldp_status ldp_server_step(ldp_server* s, int* ndone) {
 
     s->phase(0, tp);
 
-    // 2. publication: about one wave of unclaimed work per type, shortest
-    //    remaining job first
+    // 2. publication: unclaimed work kept at about what the launches in
+    //    flight and the next one will claim (slots x steps per launch x the
+    //    running jobs' mean 1 / trajectory length, per launch), shortest
+    //    remaining job first over all model types, so a job that arrives
+    //    waits behind little queued work
     bool active[4] = {false, false, false, false};
-    for (Entry* en : s->running) active[en->type] = true;
-    for (int t = 0; t < 4; ++t) {
-        if (!active[t]) continue;
-        const int64_t wave = ldp::fp32_nslots(ctx, t);
-        const unsigned long long pub = ldp::fp32_published(ctx, t);
-        int64_t backlog = (int64_t)(pub - std::min(pub, s->head_seen[t]));
-        while (backlog < wave / 2) {
+    double inv_len = 0.0;
+    for (Entry* en : s->running) {
+        active[en->type] = true;
+        inv_len += 1.0 / (double)std::max<uint64_t>(en->job->nsteps, 1);
+    }
+    if (!s->running.empty()) {
+        int64_t total = 0;
+        int64_t nslots = ldp::fp32_mixed_slots(ctx);
+        for (int t = 0; t < 4; ++t) {
+            if (!active[t]) continue;
+            const unsigned long long pub = ldp::fp32_published(ctx, t);
+            total += (int64_t)(pub - std::min(pub, s->head_seen[t]));
+            if (!nslots) nslots = ldp::fp32_nslots(ctx, t);
+        }
+        const double per_launch = (double)nslots * 2.0 * (double)s->pair_budget * inv_len /
+                                  (double)s->running.size();
+        const int64_t target = std::min<int64_t>(
+            std::max<int64_t>((int64_t)(per_launch * (s->max_inflight + 1)), 4096), 2 * nslots);
+        while (total < target) {
             Entry* best = nullptr;
             int64_t best_left = 0;
             for (Entry* en : s->running) {
-                if (en->type != t) continue;
                 const int64_t left = en->job->ntraj - en->job->fp32_published;
                 if (left > 0 && (!best || left < best_left)) { best = en; best_left = left; }
             }
             if (!best) break;
-            const int64_t chunk = std::min<int64_t>(best_left, std::max<int64_t>(wave / 2 - backlog, 1024));
-            const int e = ldp::fp32_publish_range(best->job, chunk, s->qs[t]);
+            const int64_t chunk = std::min<int64_t>(best_left, std::max<int64_t>(target - total, 1024));
+            const int e = ldp::fp32_publish_range(best->job, chunk, s->qs[best->type]);
             if (e) return fail(s, "publication", (cudaError_t)e);
-            backlog += chunk;
+            total += chunk;
         }
     }
 

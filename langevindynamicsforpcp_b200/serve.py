@@ -210,9 +210,10 @@ def run_stream(server: Server, work, arrivals, on_done=None, timeout_s: float = 
 def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: int = 24000, loads=(0.5, 0.8),
             isolated_sample: int = 24, device: int = 0, pair_budget: int = 1024, max_inflight: int = 2,
             hbm_budget: int = 0) -> dict:
-    """Capacity (every job submitted at once), isolated solve times and, per
-    offered load (a fraction of that capacity), the latency distribution of
-    a Poisson stream of the serving workload's jobs."""
+    """Capacity (every job submitted at once), the capacity the loop sustains
+    under Poisson arrivals, isolated solve times and, per offered load (a
+    fraction of the smaller capacity), the latency distribution of a
+    Poisson stream of the serving workload's jobs."""
     a = argparse.Namespace(jobs=jobs, exp_lo=exp_lo, exp_hi=exp_hi, steps=steps, loads=list(loads),
                            isolated_sample=isolated_sample)
     work = serving_workload(a.jobs, exp_lo=a.exp_lo, exp_hi=a.exp_hi, steps=a.steps)
@@ -236,6 +237,18 @@ def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: in
         out["capacity"]["host_loop"] = {
             "steps": i1["steps"] - i0["steps"], "launches": i1["launches"] - i0["launches"],
             "phase_s": [b - a for a, b in zip(i0["phase_s"], i1["phase_s"])], "phase_max_s": i1["phase_max_s"]}
+        # capacity the loop sustains under arrivals: a Poisson stream offered
+        # at the all-at-once capacity; jobs completed over the stream's wall
+        # time (when the loop falls behind, the backlog grows and this is
+        # its completion rate).  Loads below are fractions of the smaller.
+        arr = np.cumsum(np.random.default_rng(4321).exponential(1.0 / cap, size=len(work)))
+        t = time.perf_counter()
+        run_stream(srv, work, arr)
+        wall = time.perf_counter() - t
+        sustained = len(work) / wall
+        out["sustained"] = {"offered_jobs_per_s": cap, "jobs_per_s": sustained,
+                            "particle_steps_per_s": psteps / wall, "wall_s": wall}
+        base = min(cap, sustained)
         # isolated solve time: each job alone in the server (every job when
         # --isolated-sample covers them all, else a sample interpolated by
         # trajectory count within the job's model type)
@@ -257,7 +270,7 @@ def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: in
             return float(np.interp(np.log2(work[i][1]), xs[o], ys[o]))
 
         for load in a.loads:
-            rate = load * cap
+            rate = load * base
             arr = np.cumsum(np.random.default_rng(1234).exponential(1.0 / rate, size=len(work)))
             t = time.perf_counter()
             stg = np.zeros((len(work), 3))
