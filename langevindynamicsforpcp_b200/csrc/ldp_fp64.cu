@@ -728,17 +728,35 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
         named_sync(1 + u);                   // buffer u full
         if (lane == 0 && run) {
             const uint64_t s1 = (s_begin + (b + 1) * kLatBlock < s_end) ? s_begin + (b + 1) * kLatBlock : s_end;
-            for (int l = 0; s < s1; ++s, ++l) {
+            const int nl = (int)(s1 - s);
+            // the next step's Gaussian and flip schedules are loaded one step
+            // ahead, so their shared-memory latency is off the chain
+            double zn = buf.z[u][0];
+            int64_t cn0 = 0, cn1 = 0;
+            if (ETA) {
+                cn0 = buf.cand[u][0][0];
+                cn1 = buf.cand[u][1][0];
+            }
+            for (int l = 0; l < nl; ++s, ++l) {
+                const double z = zn;
+                const int64_t ca0 = cn0, ca1 = cn1;
+                if (l + 1 < nl) {
+                    zn = buf.z[u][l + 1];
+                    if (ETA) {
+                        cn0 = buf.cand[u][0][l + 1];
+                        cn1 = buf.cand[u][1][l + 1];
+                    }
+                }
                 const int64_t cell_prev = t.cell, well_prev = t.well;
                 const int lb_prev = t.lb;
-                fp64_move<OVER>(k, t, buf.z[u][l]);
+                fp64_move<OVER>(k, t, z);
                 if (t.x > blo && t.x < bhi && (int64_t)s != (int64_t)nxf) {
                     // a quiet step: same indices, no frame, no event; a flip
                     // toggles the state, takes its new schedule and the
                     // band's force for that state (the rest of the full step)
                     if (ETA && (int64_t)s == nflip) {
                         t.state ^= 1;
-                        nflip = t.state ? buf.cand[u][1][l] : buf.cand[u][0][l];
+                        nflip = t.state ? ca1 : ca0;
                         t.F = t.state ? bF1 : bF0;
                     }
                     if (t.state) ++sc1; else ++sc0;
