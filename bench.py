@@ -55,11 +55,16 @@ ACC_JOB, ACC_NTRAJ, ACC_NSTEPS, ACC_FREQSAVE = 14, 65536, 5_000_000, 2500
 # the drop-in executable runs it.  The reference took 7.133 min on 4 Xeon
 # ranks for 16 trajectories x 3e9 steps (its executed_job time.log).
 QT_STEPS, QT_FULL_STEPS, QT_REF_S = 30_000_000, 3_000_000_000, 7.133333 * 60
-# DRAM bytes per particle-step of the persistent kernel: 0.0873 B measured by
+# DRAM bytes per particle-step of the persistent kernel: 0.0870 B measured by
 # ncu with frames every 100 steps, of which the frames are 8 B per frame
-# (0.0801 B per step); the rest (0.0072 B: retire records, ring) is kept and
+# (0.0801 B per step); the rest (0.0070 B: retire records, ring) is kept and
 # the frame part scaled to this workload's frame interval.
-DRAM_BYTES_PER_STEP = 0.0072 + 8.0 / FREQSAVE
+DRAM_BYTES_PER_STEP = 0.0070 + 8.0 / FREQSAVE
+# Lane slots the persistent kernel issues per particle-step (warp
+# instructions x 32 / particle-steps), measured by ncu on one wave of the
+# bench geometry (113664 trajectories x 120000 steps, frames every 100): the
+# hot loop plus the special steps and the idle lanes of divergent ones.
+ISSUED_LANE_SLOTS_PER_STEP = 49.6
 
 
 BASE_INP = os.path.join(ROOT, "tests", "golden", "inp", "CuIDB_single__2.0_7.2_m1.0_1.00e-05.inp")
@@ -530,6 +535,8 @@ def main():
                 "kernel": "fp32_persistent_kernel<single, overdamped>",
                 "ops_per_step": OPS_PER_STEP, "kernel_ms": kms,
                 "ops_per_step_as_built": OPS_PER_STEP_AS_BUILT,
+                "issued_lane_slots_per_step_ncu": ISSUED_LANE_SLOTS_PER_STEP,
+                "issue_frac_ncu": psteps * ISSUED_LANE_SLOTS_PER_STEP / (kms * 1e-3) / 1e9 / peak_issue,
                 "frac_as_built": psteps * OPS_PER_STEP_AS_BUILT / (kms * 1e-3) / 1e9 / peak_issue,
                 "peak_basis": f"{sms} SMs x 128 lanes x {fmax:g} MHz ({fsrc})",
                 "frac_at_sampled_clock": achieved / (sms * 128 * fclk * 1e6 / 1e9)}
