@@ -21,10 +21,10 @@
 // msd_smem_f32_kernel: the same for jobs of the FP32 batched path: a
 // trajectory's frames are staged in shared memory as offsets from its first
 // frame, rounded to FP32 (an error of at most 2^-24 of the offset), the
-// displacement x[k + lag] - x[k] is taken in FP32, and its square is formed
-// and accumulated in FP64 (widened displacement, fma into FP64 32-way
-// interleaved partials of ~nframe/32 terms each), so the moment sums are
-// FP64 as on the FP64 path.  Half the shared-memory bytes per term, which
+// displacement x[k + lag] - x[k] is taken in FP32, its square is summed in
+// FP32 over groups of 8 origins per lane, and the groups' sums are
+// accumulated in FP64 (32-way interleaved partials of ~nframe/32 terms
+// each), so the moment sums are FP64 as on the FP64 path.  Half the shared-memory bytes per term, which
 // bound the FP64 kernel; with 6 lags per item, a loop without per-term
 // tests over the origins all of them have, and four blocks per SM (54 KiB
 // each) to hide the shared-load latency.  The FP64 plain path keeps the
@@ -44,6 +44,7 @@ constexpr int kMsdSmemBytes = 100 * 1024;   // two blocks per SM
 constexpr int kMsdBlock = 256;
 constexpr int kMsdLags = 4;                  // lags per work item (x[k] reuse)
 constexpr int kMsdF32SmemBytes = 54 * 1024;  // FP32 kernel: four blocks per SM
+constexpr int kMsdF32Group = 8;              // FP32 kernel: origins per FP32 partial sum
 // Lean FP32 instance (msd_smem_f32_kernel<128, 2, 16, true>), for
 // post-processing that runs beside the persistent FP32 kernel: one warp per
 // SMSP at 32 registers is what three persistent blocks leave of an SM's
@@ -145,16 +146,55 @@ __global__ void __launch_bounds__(kBlk, kMinB) msd_smem_f32_kernel(const double*
             kmax = cnt[r] > kmax ? cnt[r] : kmax;
             acc[r] = 0.0;
         }
-        // Origins every lag of the item has: no per-term test.
+        // A lag's origins k = lane + 32 i are taken in groups of kMsdF32Group
+        // (consecutive i): the squares of a group that lies wholly below the
+        // lag's origin count are summed in FP32 (at most kMsdF32Group terms,
+        // relative error below kMsdF32Group * 2^-24) and the group's sum is
+        // added to the lag's FP64 sum, one widening and one FP64 add per
+        // group instead of per term; the origins after its last whole group
+        // are added one by one in FP64.  That order depends only on the lane
+        // and the lag, not on which lags share the item, so every instance
+        // gives the same sums.
+        constexpr int kG = kMsdF32Group;
         int k = lane;
-        for (; k < kmin; k += 32) {
-            const float xk = x[k];
+        // groups whole for every lag of the item: no per-term test
+        for (; k + 32 * (kG - 1) < kmin; k += 32 * kG) {
+            float part[kNL];
+#pragma unroll
+            for (int r = 0; r < kNL; ++r) part[r] = 0.0f;
+#pragma unroll
+            for (int g = 0; g < kG; ++g) {
+                const float xk = x[k + 32 * g];
+#pragma unroll
+                for (int r = 0; r < kNL; ++r) {
+                    const float d = x[k + 32 * g + lag[r]] - xk;
+                    part[r] = fmaf(d, d, part[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kNL; ++r) acc[r] += (double)part[r];
+        }
+        // groups whole for some lags of the item
+        for (; k + 32 * (kG - 1) < kmax; k += 32 * kG) {
 #pragma unroll
             for (int r = 0; r < kNL; ++r) {
-                const double d = (double)(x[k + lag[r]] - xk);
-                acc[r] = fma(d, d, acc[r]);
+                if (k + 32 * (kG - 1) < cnt[r]) {
+                    float part = 0.0f;
+#pragma unroll
+                    for (int g = 0; g < kG; ++g) {
+                        const float d = x[k + 32 * g + lag[r]] - x[k + 32 * g];
+                        part = fmaf(d, d, part);
+                    }
+                    acc[r] += (double)part;
+                } else {
+                    for (int g = 0; g < kG && k + 32 * g < cnt[r]; ++g) {
+                        const double d = (double)(x[k + 32 * g + lag[r]] - x[k + 32 * g]);
+                        acc[r] = fma(d, d, acc[r]);
+                    }
+                }
             }
         }
+        // the origins after the last group, one by one
         for (; k < kmax; k += 32) {
             const float xk = x[k];
 #pragma unroll
