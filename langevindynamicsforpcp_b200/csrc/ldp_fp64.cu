@@ -632,9 +632,11 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
 // ---------------------------------------------------------------------------
 constexpr int kLatBlock = 32;   // steps per buffer
 
+constexpr int kLatSub = 8;       // steps per blind sub-block (see the consumer)
 struct LatBuf {
     double z[2][kLatBlock];
     int64_t cand[2][2][kLatBlock];   // [buffer][new state][step]
+    double zs[2][kLatBlock / kLatSub];   // sum of |z| over each sub-block
 };
 
 // The flip schedule of a flip at step s for both new states, from the words
@@ -685,18 +687,25 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
             const int u = (int)(b & 1);
             if (b >= 2) named_sync(3 + u);   // buffer u released by the consumer
             const uint64_t s = s_begin + b * kLatBlock + (uint64_t)lane;
+            double az = 0.0;
             if (s < s_end) {
                 const int q = (int)((s - 1) & 3);
                 const Words w = philox_at((s - 1) >> 2, g, TAG_STEP, k.key0, k.key1);
                 double za, zb;
                 if (q < 2) gauss_pair_f64(w.w0, w.w1, &za, &zb);
                 else gauss_pair_f64(w.w2, w.w3, &za, &zb);
-                buf.z[u][lane] = (q & 1) ? zb : za;
+                const double zz = (q & 1) ? zb : za;
+                buf.z[u][lane] = zz;
+                az = fabs(zz);
                 if (ETA) {
                     const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
                     flip_schedule_both(s, wf.w0, wf.w1, k.ln1m, &buf.cand[u][0][lane], &buf.cand[u][1][lane]);
                 }
             }
+            // |z| summed over each sub-block of kLatSub steps (a bound for
+            // the consumer, so its order does not matter)
+            for (int o = 1; o < kLatSub; o <<= 1) az += __shfl_xor_sync(0xffffffffu, az, o);
+            if ((lane & (kLatSub - 1)) == 0) buf.zs[u][lane / kLatSub] = az;
             __syncwarp();
             named_arrive(1 + u);             // buffer u full
         }
@@ -713,6 +722,7 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
     // quiet band (empty: the first step takes the full path) and the force
     // in it for either barrier state
     double blo = 1.0, bhi = 0.0, bF0 = 0.0, bF1 = 0.0;
+    double fmaxc = 0.0;   // largest |drift| of a step in the band, either state
     if (lane == 0) {
         load_traj(st, t, i);
         active = run = !(t.bits & B_DONE);
@@ -730,22 +740,62 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
             const uint64_t s1 = (s_begin + (b + 1) * kLatBlock < s_end) ? s_begin + (b + 1) * kLatBlock : s_end;
             const int nl = (int)(s1 - s);
             // the next step's Gaussian and flip schedules are loaded one step
-            // ahead, so their shared-memory latency is off the chain
+            // ahead, so their shared-memory latency is off the chain (zn,
+            // cn0, cn1 hold step pf's)
             double zn = buf.z[u][0];
             int64_t cn0 = 0, cn1 = 0;
             if (ETA) {
                 cn0 = buf.cand[u][0][0];
                 cn1 = buf.cand[u][1][0];
             }
-            for (int l = 0; l < nl; ++s, ++l) {
-                const double z = zn;
-                const int64_t ca0 = cn0, ca1 = cn1;
+            int pf = 0;
+            for (int l = 0; l < nl;) {
+                // Blind sub-block (overdamped): when the position is farther
+                // from both quiet-band edges than the sub-block's steps can
+                // move it -- each step at most |F| c + |r_s| + |r_{s-1}|, the
+                // |r| from the sub-block's sum of |z|, with a relative slack
+                // far above rounding -- and no frame falls in it, all its
+                // steps are quiet steps, run without the per-step band test.
+                if (OVER && (l & (kLatSub - 1)) == 0 && l + kLatSub <= nl &&
+                    (int64_t)nxf >= (int64_t)s + kLatSub) {
+                    const double bnd = ((double)kLatSub * fmaxc + k.sig_r * (2.0 * buf.zs[u][l / kLatSub]) +
+                                        fabs(t.rprev)) * (1.0 + 1e-12) + 1e-12 * (1.0 + fabs(t.x));
+                    if (t.x - bnd > blo && t.x + bnd < bhi) {
+#pragma unroll
+                        for (int m = 0; m < kLatSub; ++m) {
+                            fp64_move<OVER>(k, t, buf.z[u][l + m]);
+                            if (ETA && (int64_t)s + m == nflip) {
+                                t.state ^= 1;
+                                nflip = t.state ? buf.cand[u][1][l + m] : buf.cand[u][0][l + m];
+                                t.F = t.state ? bF1 : bF0;
+                            }
+                            if (t.state) ++sc1; else ++sc0;
+                        }
+                        s += kLatSub;
+                        l += kLatSub;
+                        continue;
+                    }
+                }
+                double z;
+                int64_t ca0 = 0, ca1 = 0;
+                if (pf == l) {
+                    z = zn;
+                    ca0 = cn0;
+                    ca1 = cn1;
+                } else {
+                    z = buf.z[u][l];
+                    if (ETA) {
+                        ca0 = buf.cand[u][0][l];
+                        ca1 = buf.cand[u][1][l];
+                    }
+                }
                 if (l + 1 < nl) {
                     zn = buf.z[u][l + 1];
                     if (ETA) {
                         cn0 = buf.cand[u][0][l + 1];
                         cn1 = buf.cand[u][1][l + 1];
                     }
+                    pf = l + 1;
                 }
                 const int64_t cell_prev = t.cell, well_prev = t.well;
                 const int lb_prev = t.lb;
@@ -761,6 +811,8 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                     }
                     if (t.state) ++sc1; else ++sc0;
                     if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+                    ++s;
+                    ++l;
                     continue;
                 }
                 const FlipFromBuffer src{&buf.cand[u][0][l], &buf.cand[u][1][l]};
@@ -770,6 +822,9 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                 if (r == 2) { ++s; run = false; break; }
                 quiet_band<DBL>(k, t, &blo, &bhi);
                 band_forces<DBL>(k, t, &bF0, &bF1);
+                fmaxc = fmax(fabs(bF0), fabs(bF1)) * fabs(k.c_drift);
+                ++s;
+                ++l;
             }
         }
         __syncwarp();
