@@ -761,15 +761,31 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                     const double bnd = ((double)kLatSub * fmaxc + k.sig_r * (2.0 * buf.zs[u][l / kLatSub]) +
                                         fabs(t.rprev)) * (1.0 + 1e-12) + 1e-12 * (1.0 + fabs(t.x));
                     if (t.x - bnd > blo && t.x + bnd < bhi) {
+                        // the sub-block's draws into registers first; flips
+                        // by selects (t.F is the band's force of the state
+                        // throughout), so the steps form one chain in x
+                        double zb[kLatSub];
+                        int64_t c0b[kLatSub], c1b[kLatSub];
 #pragma unroll
                         for (int m = 0; m < kLatSub; ++m) {
-                            fp64_move<OVER>(k, t, buf.z[u][l + m]);
-                            if (ETA && (int64_t)s + m == nflip) {
-                                t.state ^= 1;
-                                nflip = t.state ? buf.cand[u][1][l + m] : buf.cand[u][0][l + m];
+                            zb[m] = buf.z[u][l + m];
+                            if (ETA) {
+                                c0b[m] = buf.cand[u][0][l + m];
+                                c1b[m] = buf.cand[u][1][l + m];
+                            }
+                        }
+#pragma unroll
+                        for (int m = 0; m < kLatSub; ++m) {
+                            fp64_move<OVER>(k, t, zb[m]);
+                            if (ETA) {
+                                const bool f = (int64_t)s + m == nflip;
+                                t.state ^= (int)f;
+                                const int64_t cn = t.state ? c1b[m] : c0b[m];
+                                nflip = f ? cn : nflip;
                                 t.F = t.state ? bF1 : bF0;
                             }
-                            if (t.state) ++sc1; else ++sc0;
+                            sc1 += t.state;
+                            sc0 += 1 - t.state;
                         }
                         s += kLatSub;
                         l += kLatSub;
