@@ -632,11 +632,10 @@ __global__ void __launch_bounds__(128, 4) fp64_steps_kernel(const KConst k, cons
 // ---------------------------------------------------------------------------
 constexpr int kLatBlock = 32;   // steps per buffer
 
-constexpr int kLatSub = 8;       // steps per blind sub-block (see the consumer)
+constexpr int kLatSub = 8;       // steps per speculative sub-block (see the consumer)
 struct LatBuf {
     double z[2][kLatBlock];
     int64_t cand[2][2][kLatBlock];   // [buffer][new state][step]
-    double zs[2][kLatBlock / kLatSub];   // sum of |z| over each sub-block
 };
 
 // The flip schedule of a flip at step s for both new states, from the words
@@ -687,25 +686,18 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
             const int u = (int)(b & 1);
             if (b >= 2) named_sync(3 + u);   // buffer u released by the consumer
             const uint64_t s = s_begin + b * kLatBlock + (uint64_t)lane;
-            double az = 0.0;
             if (s < s_end) {
                 const int q = (int)((s - 1) & 3);
                 const Words w = philox_at((s - 1) >> 2, g, TAG_STEP, k.key0, k.key1);
                 double za, zb;
                 if (q < 2) gauss_pair_f64(w.w0, w.w1, &za, &zb);
                 else gauss_pair_f64(w.w2, w.w3, &za, &zb);
-                const double zz = (q & 1) ? zb : za;
-                buf.z[u][lane] = zz;
-                az = fabs(zz);
+                buf.z[u][lane] = (q & 1) ? zb : za;
                 if (ETA) {
                     const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
                     flip_schedule_both(s, wf.w0, wf.w1, k.ln1m, &buf.cand[u][0][lane], &buf.cand[u][1][lane]);
                 }
             }
-            // |z| summed over each sub-block of kLatSub steps (a bound for
-            // the consumer, so its order does not matter)
-            for (int o = 1; o < kLatSub; o <<= 1) az += __shfl_xor_sync(0xffffffffu, az, o);
-            if ((lane & (kLatSub - 1)) == 0) buf.zs[u][lane / kLatSub] = az;
             __syncwarp();
             named_arrive(1 + u);             // buffer u full
         }
@@ -722,7 +714,6 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
     // quiet band (empty: the first step takes the full path) and the force
     // in it for either barrier state
     double blo = 1.0, bhi = 0.0, bF0 = 0.0, bF1 = 0.0;
-    double fmaxc = 0.0;   // largest |drift| of a step in the band, either state
     if (lane == 0) {
         load_traj(st, t, i);
         active = run = !(t.bits & B_DONE);
@@ -750,47 +741,62 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
             }
             int pf = 0;
             for (int l = 0; l < nl;) {
-                // Blind sub-block (overdamped): when the position is farther
-                // from both quiet-band edges than the sub-block's steps can
-                // move it -- each step at most |F| c + |r_s| + |r_{s-1}|, the
-                // |r| from the sub-block's sum of |z|, with a relative slack
-                // far above rounding -- and no frame falls in it, all its
-                // steps are quiet steps, run without the per-step band test.
-                if (OVER && (l & (kLatSub - 1)) == 0 && l + kLatSub <= nl &&
-                    (int64_t)nxf >= (int64_t)s + kLatSub) {
-                    const double bnd = ((double)kLatSub * fmaxc + k.sig_r * (2.0 * buf.zs[u][l / kLatSub]) +
-                                        fabs(t.rprev)) * (1.0 + 1e-12) + 1e-12 * (1.0 + fabs(t.x));
-                    if (t.x - bnd > blo && t.x + bnd < bhi) {
-                        // the sub-block's draws into registers first; flips
-                        // by selects (t.F is the band's force of the state
-                        // throughout), so the steps form one chain in x
-                        double zb[kLatSub];
-                        int64_t c0b[kLatSub], c1b[kLatSub];
+                // Speculative sub-block: the next kLatSub steps run as quiet
+                // steps without the per-step band test, keeping the lowest
+                // and highest position; when every position stayed inside
+                // the quiet band (and no frame falls in the sub-block) they
+                // were quiet steps and stand, else the state at the
+                // sub-block's start is restored and the steps run one by one.
+                // x turning NaN stays NaN to the end, which the final test
+                // catches.
+                if (l + kLatSub <= nl && (l & (kLatSub - 1)) == 0 && (int64_t)nxf >= (int64_t)s + kLatSub &&
+                    t.x > blo && t.x < bhi) {
+                    double zb[kLatSub];
+                    int64_t c0b[kLatSub], c1b[kLatSub];
 #pragma unroll
-                        for (int m = 0; m < kLatSub; ++m) {
-                            zb[m] = buf.z[u][l + m];
-                            if (ETA) {
-                                c0b[m] = buf.cand[u][0][l + m];
-                                c1b[m] = buf.cand[u][1][l + m];
-                            }
+                    for (int m = 0; m < kLatSub; ++m) {
+                        zb[m] = buf.z[u][l + m];
+                        if (ETA) {
+                            c0b[m] = buf.cand[u][0][l + m];
+                            c1b[m] = buf.cand[u][1][l + m];
                         }
+                    }
+                    const double x0 = t.x, v0 = t.v, F0 = t.F, r0 = t.rprev;
+                    const int st0 = t.state;
+                    const int64_t nflip0 = nflip, sc00 = sc0, sc10 = sc1;
+                    double xmin = t.x, xmax = t.x;
 #pragma unroll
-                        for (int m = 0; m < kLatSub; ++m) {
-                            fp64_move<OVER>(k, t, zb[m]);
-                            if (ETA) {
-                                const bool f = (int64_t)s + m == nflip;
-                                t.state ^= (int)f;
-                                const int64_t cn = t.state ? c1b[m] : c0b[m];
-                                nflip = f ? cn : nflip;
-                                t.F = t.state ? bF1 : bF0;
-                            }
-                            sc1 += t.state;
-                            sc0 += 1 - t.state;
+                    for (int m = 0; m < kLatSub; ++m) {
+                        fp64_move<OVER>(k, t, zb[m]);
+                        xmin = fmin(xmin, t.x);
+                        xmax = fmax(xmax, t.x);
+                        if (ETA) {
+                            // flips by selects (t.F is the band's force of
+                            // the state throughout), so the steps form one
+                            // chain in x
+                            const bool f = (int64_t)s + m == nflip;
+                            t.state ^= (int)f;
+                            const int64_t cn = t.state ? c1b[m] : c0b[m];
+                            nflip = f ? cn : nflip;
+                            t.F = t.state ? bF1 : bF0;
                         }
+                        sc1 += t.state;
+                        sc0 += 1 - t.state;
+                        if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+                    }
+                    if (xmin > blo && xmax < bhi && t.x > blo) {
                         s += kLatSub;
                         l += kLatSub;
                         continue;
                     }
+                    t.x = x0;
+                    t.v = v0;
+                    t.F = F0;
+                    t.rprev = r0;
+                    t.state = st0;
+                    nflip = nflip0;
+                    sc0 = sc00;
+                    sc1 = sc10;
                 }
                 double z;
                 int64_t ca0 = 0, ca1 = 0;
@@ -838,7 +844,6 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                 if (r == 2) { ++s; run = false; break; }
                 quiet_band<DBL>(k, t, &blo, &bhi);
                 band_forces<DBL>(k, t, &bF0, &bF1);
-                fmaxc = fmax(fabs(bF0), fabs(bF1)) * fabs(k.c_drift);
                 ++s;
                 ++l;
             }
