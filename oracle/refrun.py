@@ -1,6 +1,6 @@
 """Runs the CPU-baseline build of the reference's own code (oracle/_ref).
 
-TEST AND BASELINE INFRASTRUCTURE ONLY: imported by tests/ (statistical
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: imported by tests/ (statistical
 checks of the device paths against the reference's code) and by bench.py's
 reference arm and cpu_baseline leg (the reference's CPU path timed on the
 host cores).  It imports nothing of the product.
