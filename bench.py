@@ -294,7 +294,7 @@ def serving_leg(device):
         out["loads"][load] = {k: v[k] for k in ("rate_jobs_per_s", "p50_latency_s", "p99_latency_s",
                                                 "p50_over_isolated", "p99_over_isolated",
                                                 "p99_latency_over_p99_isolated", "particle_steps_per_s",
-                                                "by_trajectory_count", "p99_stage_s")}
+                                                "by_trajectory_count", "p50_stage_s", "p99_stage_s")}
     return out
 
 

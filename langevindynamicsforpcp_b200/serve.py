@@ -295,6 +295,9 @@ def measure(jobs: int = 10000, exp_lo: float = 10, exp_hi: float = 18, steps: in
                 # each), beside the per-job ratio above
                 "p99_latency_over_p99_isolated": float(np.percentile(lat, 99) / np.percentile(iso_all, 99)),
                 "particle_steps_per_s": psteps / wall,
+                "p50_stage_s": {"queued": float(np.percentile(stg[:, 0], 50)),
+                                "integrating": float(np.percentile(stg[:, 1] - stg[:, 0], 50)),
+                                "post_processing": float(np.percentile(stg[:, 2] - stg[:, 1], 50))},
                 "p99_stage_s": {"queued": float(np.percentile(stg[:, 0], 99)),
                                 "integrating": float(np.percentile(stg[:, 1] - stg[:, 0], 99)),
                                 "post_processing": float(np.percentile(stg[:, 2] - stg[:, 1], 99))},
