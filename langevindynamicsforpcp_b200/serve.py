@@ -2,8 +2,9 @@
 
 Jobs (.inp parameter sets) arrive over time; the C++ serving loop admits
 them by device-memory footprint, runs them in the shared persistent launches
-of their model type while other jobs are in flight (continuous batching) and
-finishes each one as soon as its trajectories have all retired.  This module
+(one launch covers every model type) while other jobs are in flight
+(continuous batching) and finishes each one as soon as its trajectories have
+all retired.  This module
 adds the request side: a Poisson arrival stream, per-job latency, and the
 "serving" workload -- jobs of random type (single or double barrier, under-
 or overdamped), parameters from the precision / batching / scan ranges,
@@ -84,6 +85,7 @@ class Server:
         h = C.c_void_p()
         _check(L.lib().ldp_server_create(ctx.handle, C.byref(o), C.byref(h)), ctx)
         self.handle = h
+        self._ended = (C.c_uint64 * 4096)()
 
     def submit(self, params, lanes: int, job_id: int = 0) -> int:
         o = L.JobOpts()
@@ -103,9 +105,10 @@ class Server:
         _check(L.lib().ldp_server_poll(self.handle, ticket, C.byref(st), C.byref(lat)), self.ctx)
         return st.value, lat.value
 
-    def ended(self, cap: int = 4096) -> list:
+    def ended(self) -> list:
         """Tickets of the jobs that ended (done or failed) since the last call."""
-        buf = (C.c_uint64 * cap)()
+        buf = self._ended
+        cap = len(buf)
         n = C.c_int64(0)
         out = []
         while True:
