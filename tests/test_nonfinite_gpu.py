@@ -28,7 +28,7 @@ def params(overdamped, temperature):
 
 
 @pytest.mark.parametrize("overdamped", [1, 0])
-@pytest.mark.parametrize("latency", [2048, 0])
+@pytest.mark.parametrize("latency", [4096, 0])
 def test_fp64_nonfinite_trajectories_freeze_as_the_oracle(overdamped, latency):
     p = params(overdamped, -1.0)
     with ldp.Context(0) as ctx:

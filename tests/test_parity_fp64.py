@@ -57,7 +57,7 @@ def ctx_thread():
 @pytest.fixture(scope="module", params=["latency", "thread"])
 def ctx(request, ctx_thread):
     # Every parity case runs twice: small jobs in latency mode (a CTA per
-    # trajectory, the default below 2048 trajectories) and with one
+    # trajectory, the default up to 4096 trajectories) and with one
     # trajectory per thread; both must equal the oracle bit for bit.
     if request.param == "thread":
         return ctx_thread
