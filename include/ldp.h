@@ -264,8 +264,15 @@ ldp_status  ldp_ctx_synchronize(ldp_ctx *ctx);
  * integrates, for runs of few long trajectories (the reference's sample:
  * 16-32 trajectories x 3e9 steps), whose per-step dependency chain bounds
  * them.  Results are the same bit for bit either way.  0 disables it;
- * default 4096.  No reference counterpart. */
+ * default 2048.  No reference counterpart. */
 ldp_status  ldp_ctx_set_fp64_latency(ldp_ctx *ctx, int64_t max_traj);
+/* FP64 plain fixed-step jobs above the latency-mode limit and of at most
+ * max_traj trajectories run in group mode: a CTA of 32 trajectories, a
+ * consumer warp stepping them (lane l one trajectory) while producer warps
+ * draw their Gaussians and flip schedules ahead, for runs of a few thousand
+ * trajectories.  Results are the same bit for bit.  0 disables it;
+ * default 16384.  No reference counterpart. */
+ldp_status  ldp_ctx_set_fp64_group(ldp_ctx *ctx, int64_t max_traj);
 /* The shape in effect: the resolved values once the first FP32 job ran. */
 ldp_status  ldp_ctx_get_fp32_shape(ldp_ctx *ctx, int *block, int *grid, uint64_t *pair_budget,
                                    int *ring_slots);

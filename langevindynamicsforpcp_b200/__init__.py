@@ -73,6 +73,14 @@ class Context:
         if st != 0:
             raise LdpError(st, "ldp_ctx_set_fp64_latency")
 
+    def set_fp64_group(self, max_traj: int) -> None:
+        """FP64 plain fixed-step jobs above the latency-mode limit and with at
+        most max_traj trajectories run in group mode (ldp_ctx_set_fp64_group;
+        0 disables it)."""
+        st = L.lib().ldp_ctx_set_fp64_group(self.handle, max_traj)
+        if st != 0:
+            raise LdpError(st, "ldp_ctx_set_fp64_group")
+
     def close(self):
         if self.handle:
             L.lib().ldp_destroy(self.handle)

@@ -167,6 +167,7 @@ SIGNATURES = {
     "ldp_server_info_get": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
     "ldp_server_destroy": (None, [C.c_void_p]),
     "ldp_ctx_set_fp64_latency": (C.c_int, [C.c_void_p, C.c_int64]),
+    "ldp_ctx_set_fp64_group": (C.c_int, [C.c_void_p, C.c_int64]),
     "ldp_job_keep_state": (C.c_int, [C.c_void_p]),
     "ldp_job_save_state": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ldp_job_load_state": (C.c_int, [C.c_void_p, C.c_char_p]),

@@ -80,5 +80,9 @@ int launch_fp64_steps(const KConst& k, const TrajState& st, int64_t g0, uint64_t
 // warp per trajectory, the same results bit for bit.
 int launch_fp64_latency(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end,
                         void* stream);
+// Group mode: a CTA of 32 trajectories, producer warps drawing ahead of a
+// consumer warp (same results bit for bit).
+int launch_fp64_group(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end,
+                        void* stream);
 
 }  // namespace ldp

@@ -863,6 +863,232 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
     store_traj(st, t, i);
 }
 
+// ---------------------------------------------------------------------------
+// Group mode: mid-size runs (a few thousand trajectories).  Latency mode
+// gives each trajectory a CTA and saturates near 7e9 particle-steps/s; one
+// trajectory per thread leaves a few warps per SM, each waiting on its own
+// draws.  Here a CTA runs 32 trajectories: a consumer warp, lane l the
+// trajectory 32 blockIdx + l, steps them with latency mode's consumer code
+// (quiet steps, speculative sub-blocks, full steps through fp64_after_move),
+// and kGrpProducers producer warps draw their Gaussians and flip schedules
+// for the next kGrpBlock steps into shared memory (producer lane p: the
+// trajectory p mod 32, steps p / 32, p / 32 + kGrpProducers, ... of the
+// block).  Two buffers alternate, handed over with named barriers 5-6
+// ("full") and 7-8 ("empty") over all the CTA's warps; every arrival is
+// matched by one wait, with no spin loop.  Same inputs, same operations:
+// results equal the other kernels' and the oracle's bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kGrpBlock = 16;      // steps per buffer
+constexpr int kGrpProducers = 4;   // producer warps per CTA
+constexpr int kGrpThreads = 32 * (1 + kGrpProducers);
+struct GrpBuf {
+    double z[2][kGrpBlock][32];          // [buffer][step][trajectory]
+    int64_t cand[2][2][kGrpBlock][32];   // [buffer][new state][step][trajectory]
+};
+
+__device__ __forceinline__ void grp_sync(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kGrpThreads) : "memory");
+}
+__device__ __forceinline__ void grp_arrive(int id) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "n"(kGrpThreads) : "memory");
+}
+
+template <bool DBL, bool OVER, bool ETA>
+__global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst k, const TrajState st, int64_t g0,
+                                                                    uint64_t s_begin, uint64_t s_end) {
+    __shared__ GrpBuf buf;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t nblk = (s_end > s_begin) ? (s_end - s_begin + kGrpBlock - 1) / kGrpBlock : 0;
+    if (warp >= 1) {
+        // ---- producers ----
+        const int p = (warp - 1) * 32 + lane;
+        const int tl = p & 31;               // the trajectory's lane
+        const int64_t ip = (int64_t)blockIdx.x * 32 + tl;
+        const uint32_t g = (uint32_t)(g0 + ip);
+        for (uint64_t b = 0; b < nblk; ++b) {
+            const int u = (int)(b & 1);
+            if (b >= 2) grp_sync(7 + u);     // buffer u released by the consumer
+            for (int e = p >> 5; e < kGrpBlock; e += kGrpProducers) {
+                const uint64_t s = s_begin + b * kGrpBlock + (uint64_t)e;
+                if (ip >= st.n || s >= s_end) continue;
+                const int q = (int)((s - 1) & 3);
+                const Words w = philox_at((s - 1) >> 2, g, TAG_STEP, k.key0, k.key1);
+                double za, zb;
+                if (q < 2) gauss_pair_f64(w.w0, w.w1, &za, &zb);
+                else gauss_pair_f64(w.w2, w.w3, &za, &zb);
+                buf.z[u][e][tl] = (q & 1) ? zb : za;
+                if (ETA) {
+                    const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
+                    flip_schedule_both(s, wf.w0, wf.w1, k.ln1m, &buf.cand[u][0][e][tl], &buf.cand[u][1][e][tl]);
+                }
+            }
+            __syncwarp();
+            grp_arrive(5 + u);               // buffer u full
+        }
+        // the consumer's release of the last two buffers
+        for (uint64_t b = (nblk > 2 ? nblk - 2 : 0); b < nblk; ++b) grp_sync(7 + (int)(b & 1));
+        return;
+    }
+    // ---- consumer: lane l runs trajectory 32 blockIdx + l ----
+    const int64_t i = (int64_t)blockIdx.x * 32 + lane;
+    const uint32_t g = (uint32_t)(g0 + i);
+    T64 t;
+    int64_t sc0 = 0, sc1 = 0, nflip = 0;
+    uint32_t flags = 0;
+    uint64_t s = s_begin, nxf = 0;
+    bool run = false, active = false;
+    // quiet band (empty: the first step takes the full path) and the force
+    // in it for either barrier state
+    double blo = 1.0, bhi = 0.0, bF0 = 0.0, bF1 = 0.0;
+    if (i < st.n) {
+        load_traj(st, t, i);
+        active = run = !(t.bits & B_DONE);
+        sc0 = st.counts[(int64_t)LDP_C_STATE0 * st.n + i];
+        sc1 = st.counts[(int64_t)LDP_C_STATE1 * st.n + i];
+        energy_force<DBL>(k, t);
+        nflip = st.nflip[i];
+        const uint64_t fs = k.freq_save;
+        nxf = (s_begin + fs - 1) / fs * fs;
+    }
+    for (uint64_t b = 0; b < nblk; ++b) {
+        const int u = (int)(b & 1);
+        grp_sync(5 + u);                     // buffer u full
+        if (run) {
+            const uint64_t s1 = (s_begin + (b + 1) * kGrpBlock < s_end) ? s_begin + (b + 1) * kGrpBlock : s_end;
+            const int nl = (int)(s1 - s);
+            // the next step's Gaussian and flip schedules are loaded one step
+            // ahead, so their shared-memory latency is off the chain (zn,
+            // cn0, cn1 hold step pf's)
+            double zn = buf.z[u][0][lane];
+            int64_t cn0 = 0, cn1 = 0;
+            if (ETA) {
+                cn0 = buf.cand[u][0][0][lane];
+                cn1 = buf.cand[u][1][0][lane];
+            }
+            int pf = 0;
+            for (int l = 0; l < nl;) {
+                // Speculative sub-block: the next kLatSub steps run as quiet
+                // steps without the per-step band test, keeping the lowest
+                // and highest position; when every position stayed inside
+                // the quiet band (and no frame falls in the sub-block) they
+                // were quiet steps and stand, else the state at the
+                // sub-block's start is restored and the steps run one by one.
+                // x turning NaN stays NaN to the end, which the final test
+                // catches.
+                if (l + kLatSub <= nl && (l & (kLatSub - 1)) == 0 && (int64_t)nxf >= (int64_t)s + kLatSub &&
+                    t.x > blo && t.x < bhi) {
+                    double zb[kLatSub];
+                    int64_t c0b[kLatSub], c1b[kLatSub];
+#pragma unroll
+                    for (int m = 0; m < kLatSub; ++m) {
+                        zb[m] = buf.z[u][l + m][lane];
+                        if (ETA) {
+                            c0b[m] = buf.cand[u][0][l + m][lane];
+                            c1b[m] = buf.cand[u][1][l + m][lane];
+                        }
+                    }
+                    const double x0 = t.x, v0 = t.v, F0 = t.F, r0 = t.rprev;
+                    const int st0 = t.state;
+                    const int64_t nflip0 = nflip, sc00 = sc0, sc10 = sc1;
+                    double xmin = t.x, xmax = t.x;
+#pragma unroll
+                    for (int m = 0; m < kLatSub; ++m) {
+                        fp64_move<OVER>(k, t, zb[m]);
+                        xmin = fmin(xmin, t.x);
+                        xmax = fmax(xmax, t.x);
+                        if (ETA) {
+                            // flips by selects (t.F is the band's force of
+                            // the state throughout), so the steps form one
+                            // chain in x
+                            const bool f = (int64_t)s + m == nflip;
+                            t.state ^= (int)f;
+                            const int64_t cn = t.state ? c1b[m] : c0b[m];
+                            nflip = f ? cn : nflip;
+                            t.F = t.state ? bF1 : bF0;
+                        }
+                        sc1 += t.state;
+                        sc0 += 1 - t.state;
+                        if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+                    }
+                    if (xmin > blo && xmax < bhi && t.x > blo) {
+                        s += kLatSub;
+                        l += kLatSub;
+                        continue;
+                    }
+                    t.x = x0;
+                    t.v = v0;
+                    t.F = F0;
+                    t.rprev = r0;
+                    t.state = st0;
+                    nflip = nflip0;
+                    sc0 = sc00;
+                    sc1 = sc10;
+                }
+                double z;
+                int64_t ca0 = 0, ca1 = 0;
+                if (pf == l) {
+                    z = zn;
+                    ca0 = cn0;
+                    ca1 = cn1;
+                } else {
+                    z = buf.z[u][l][lane];
+                    if (ETA) {
+                        ca0 = buf.cand[u][0][l][lane];
+                        ca1 = buf.cand[u][1][l][lane];
+                    }
+                }
+                if (l + 1 < nl) {
+                    zn = buf.z[u][l + 1][lane];
+                    if (ETA) {
+                        cn0 = buf.cand[u][0][l + 1][lane];
+                        cn1 = buf.cand[u][1][l + 1][lane];
+                    }
+                    pf = l + 1;
+                }
+                const int64_t cell_prev = t.cell, well_prev = t.well;
+                const int lb_prev = t.lb;
+                fp64_move<OVER>(k, t, z);
+                if (t.x > blo && t.x < bhi && (int64_t)s != (int64_t)nxf) {
+                    // a quiet step: same indices, no frame, no event; a flip
+                    // toggles the state, takes its new schedule and the
+                    // band's force for that state (the rest of the full step)
+                    if (ETA && (int64_t)s == nflip) {
+                        t.state ^= 1;
+                        nflip = t.state ? ca1 : ca0;
+                        t.F = t.state ? bF1 : bF0;
+                    }
+                    if (t.state) ++sc1; else ++sc0;
+                    if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
+                    ++s;
+                    ++l;
+                    continue;
+                }
+                const FlipFromBuffer src{&buf.cand[u][0][l][lane], &buf.cand[u][1][l][lane]};
+                const int r = fp64_after_move<DBL, OVER, ETA>(k, st, i, g, t, s, src, nflip, sc0, sc1, flags, nxf,
+                                                              cell_prev, well_prev, lb_prev);
+                if (r == 1) { run = false; break; }
+                if (r == 2) { ++s; run = false; break; }
+                quiet_band<DBL>(k, t, &blo, &bhi);
+                band_forces<DBL>(k, t, &bF0, &bF1);
+                ++s;
+                ++l;
+            }
+        }
+        __syncwarp();
+        grp_arrive(7 + u);                   // buffer u released
+    }
+    if (!active) return;   // a trajectory done before the launch keeps its state
+    // s is the first step not integrated
+    const int64_t n = st.n;
+    st.counts[(int64_t)LDP_C_STATE0 * n + i] = sc0;
+    st.counts[(int64_t)LDP_C_STATE1 * n + i] = sc1;
+    st.counts[(int64_t)LDP_C_STEPS * n + i] = (int64_t)s - 1;
+    if (k.fp_mode && !(t.bits & B_DONE) && s_end > k.step_cap) flags |= LDP_FLAG_CENSORED;
+    if (flags) st.counts[(int64_t)LDP_C_FLAGS * n + i] |= (int64_t)flags;
+    st.nflip[i] = nflip;
+    store_traj(st, t, i);
+}
+
 template <bool DBL, bool OVER>
 static int launch_init_t(const KConst& k, const TrajState& st, int64_t g0, int block, cudaStream_t stream) {
     const int64_t grid = (st.n + block - 1) / block;
@@ -906,6 +1132,31 @@ int launch_fp64_latency(const KConst& k, const TrajState& st, int64_t g0, uint64
         case 5: return launch_latency_t<true, false, true>(k, st, g0, s_begin, s_end, s);
         case 6: return launch_latency_t<true, true, false>(k, st, g0, s_begin, s_end, s);
         default: return launch_latency_t<true, true, true>(k, st, g0, s_begin, s_end, s);
+    }
+}
+
+template <bool DBL, bool OVER, bool ETA>
+static int launch_group_t(const KConst& k, const TrajState& st, int64_t g0, uint64_t s0, uint64_t s1,
+                          cudaStream_t stream) {
+    const int64_t grid = (st.n + 31) / 32;
+    fp64_group_kernel<DBL, OVER, ETA><<<(unsigned)grid, kGrpThreads, 0, stream>>>(k, st, g0, s0, s1);
+    return (int)cudaGetLastError();
+}
+
+int launch_fp64_group(const KConst& k, const TrajState& st, int64_t g0, uint64_t s_begin, uint64_t s_end,
+                      void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (st.n <= 0) return 0;
+    const int sel = (k.dbl ? 4 : 0) | (k.over ? 2 : 0) | (k.eta ? 1 : 0);
+    switch (sel) {
+        case 0: return launch_group_t<false, false, false>(k, st, g0, s_begin, s_end, s);
+        case 1: return launch_group_t<false, false, true>(k, st, g0, s_begin, s_end, s);
+        case 2: return launch_group_t<false, true, false>(k, st, g0, s_begin, s_end, s);
+        case 3: return launch_group_t<false, true, true>(k, st, g0, s_begin, s_end, s);
+        case 4: return launch_group_t<true, false, false>(k, st, g0, s_begin, s_end, s);
+        case 5: return launch_group_t<true, false, true>(k, st, g0, s_begin, s_end, s);
+        case 6: return launch_group_t<true, true, false>(k, st, g0, s_begin, s_end, s);
+        default: return launch_group_t<true, true, true>(k, st, g0, s_begin, s_end, s);
     }
 }
 

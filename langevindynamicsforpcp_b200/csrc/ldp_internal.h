@@ -16,10 +16,14 @@ struct Fp32Runtime;
 constexpr int kCtxMarks = 16;
 constexpr int kCtxF64Streams = 2;   // streams FP64 plain jobs of a batch share
 // FP64 plain fixed-step jobs of at most this many trajectories run in
-// latency mode (a CTA per trajectory) by default: on the reference's sample
-// shape it gives 7.3e9 particle-steps/s from 2048 trajectories on, against
-// 4.4e9 for one trajectory per thread at 4096 and 8.8e9 at 8192.
-constexpr int64_t kFp64LatencyMaxTraj = 4096;
+// latency mode (a CTA per trajectory) by default, jobs above that and up to
+// kFp64GroupMaxTraj in group mode (32 trajectories per CTA with producer
+// warps), larger ones one trajectory per thread.  On the reference's sample
+// shape (particle-steps/s): 1024 trajectories 6.2e9 / 2.6e9 / 1.1e9
+// (latency / group / thread), 4096: 7.2e9 / 1.04e10 / 4.4e9, 8192: 7.3e9 /
+// 1.86e10 / 8.7e9, 16384: - / 1.88e10 / 1.73e10, 32768: - / 1.93e10 / 3.07e10.
+constexpr int64_t kFp64LatencyMaxTraj = 2048;
+constexpr int64_t kFp64GroupMaxTraj = 16384;
 
 struct ldp_ctx {
     cudaEvent_t marks[kCtxMarks] = {};   // ldp_ctx_mark / ldp_ctx_elapsed_ms
@@ -35,6 +39,7 @@ struct ldp_ctx {
     uint64_t fp32_pair_budget = 0; // step pairs per slot per launch (0: default)
     int fp32_ring_slots = 0;       // cell-table ring slots per slot (0: default 64)
     int64_t fp64_latency_max = kFp64LatencyMaxTraj;   // latency mode up to this many trajectories
+    int64_t fp64_group_max = kFp64GroupMaxTraj;       // then group mode up to this many
     cudaStream_t side = nullptr;   // post-processing beside running batches (high priority)
     cudaStream_t rd = nullptr;     // result reads of finished jobs, beside running work
     cudaStream_t gside = nullptr;  // side branch captured into batch graphs

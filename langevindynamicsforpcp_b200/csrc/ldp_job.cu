@@ -556,10 +556,13 @@ static ldp_status submit_on(ldp_ctx* ctx, ldp_job* job, cudaStream_t s) {
         const uint64_t spl = auto_steps_per_launch(job);
         const uint64_t first = job->steps_before + 1, last = job->steps_before + job->nsteps;
         // Few trajectories: latency mode (same results bit for bit).
-        const bool latency = job->o.mode == LDP_MODE_FIXED_STEPS && job->ntraj <= ctx->fp64_latency_max;
+        const bool fixed = job->o.mode == LDP_MODE_FIXED_STEPS;
+        const bool latency = fixed && job->ntraj <= ctx->fp64_latency_max;
+        const bool group = fixed && !latency && job->ntraj <= ctx->fp64_group_max;
         for (uint64_t s0 = first; s0 <= last; s0 += spl) {
             const uint64_t s1 = std::min<uint64_t>(s0 + spl, last + 1);
             e = latency ? launch_fp64_latency(job->k, job->st, job->k.g0, s0, s1, s)
+                : group ? launch_fp64_group(job->k, job->st, job->k.g0, s0, s1, s)
                         : launch_fp64_steps(job->k, job->st, job->k.g0, s0, s1, job->o.block_size, s);
             if (e) {
                 ldp_set_error(ctx, "step launch failed: %s", cudaGetErrorString((cudaError_t)e));
@@ -585,6 +588,12 @@ static ldp_status submit_on(ldp_ctx* ctx, ldp_job* job, cudaStream_t s) {
 extern "C" ldp_status ldp_ctx_set_fp64_latency(ldp_ctx* ctx, int64_t max_traj) {
     if (!ctx || max_traj < 0) return LDP_ERR_INVALID;
     ctx->fp64_latency_max = max_traj;
+    return LDP_OK;
+}
+
+extern "C" ldp_status ldp_ctx_set_fp64_group(ldp_ctx* ctx, int64_t max_traj) {
+    if (!ctx || max_traj < 0) return LDP_ERR_INVALID;
+    ctx->fp64_group_max = max_traj;
     return LDP_OK;
 }
 

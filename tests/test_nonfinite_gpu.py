@@ -3,9 +3,9 @@
 The model's forces are bounded, so no valid input blows up; a negative
 TEMPERATURE makes the noise amplitude NaN, which turns every position NaN at
 its first step.  Such a trajectory is frozen with LDP_FLAG_NONFINITE (its
-steps stop counting), on every path: FP64 (latency mode and one trajectory
-per thread) equal the oracle exactly, FP32 batched sets the same flag and
-counts, and the other trajectories of the batch are unaffected.
+steps stop counting), on every path: FP64 equals the oracle exactly, FP32 batched sets the same flag and
+counts, and the other trajectories of the batch are unaffected.  FP64 runs
+in all three kernels (latency mode, group mode, one trajectory per thread).
 """
 import os
 
@@ -28,11 +28,12 @@ def params(overdamped, temperature):
 
 
 @pytest.mark.parametrize("overdamped", [1, 0])
-@pytest.mark.parametrize("latency", [4096, 0])
-def test_fp64_nonfinite_trajectories_freeze_as_the_oracle(overdamped, latency):
+@pytest.mark.parametrize("latency,group", [(4096, 0), (0, 1 << 30), (0, 0)])   # latency / group / thread
+def test_fp64_nonfinite_trajectories_freeze_as_the_oracle(overdamped, latency, group):
     p = params(overdamped, -1.0)
     with ldp.Context(0) as ctx:
         ctx.set_fp64_latency(latency)
+        ctx.set_fp64_group(group)
         with ldp.Job(ctx, p, lanes=8, ranks=2, table_slots=256) as job:
             job.run()
             dev = job.results()

@@ -47,20 +47,34 @@ def double(steps=120_000, freq=40, **kw):
 
 @pytest.fixture(scope="module")
 def ctx_thread():
-    # a context whose FP64 jobs never use latency mode
+    # a context whose FP64 jobs run one trajectory per thread
     c = ldp.Context(0)
     c.set_fp64_latency(0)
+    c.set_fp64_group(0)
     yield c
     c.close()
 
 
-@pytest.fixture(scope="module", params=["latency", "thread"])
+@pytest.fixture(scope="module")
+def ctx_group():
+    # a context whose FP64 jobs all run in group mode
+    c = ldp.Context(0)
+    c.set_fp64_latency(0)
+    c.set_fp64_group(1 << 30)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module", params=["latency", "thread", "group"])
 def ctx(request, ctx_thread):
-    # Every parity case runs twice: small jobs in latency mode (a CTA per
-    # trajectory, the default up to 4096 trajectories) and with one
-    # trajectory per thread; both must equal the oracle bit for bit.
+    # Every parity case runs three times: small jobs in latency mode (a CTA
+    # per trajectory, the default up to 2048 trajectories), with one
+    # trajectory per thread, and in group mode (32 trajectories per CTA with
+    # producer warps); all must equal the oracle bit for bit.
     if request.param == "thread":
         return ctx_thread
+    if request.param == "group":
+        return request.getfixturevalue("ctx_group")
     c = request.getfixturevalue("ctx_default")
     return c
 
