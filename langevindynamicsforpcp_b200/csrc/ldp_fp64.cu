@@ -872,8 +872,9 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
 // (quiet steps, speculative sub-blocks, full steps through fp64_after_move),
 // and kGrpProducers producer warps draw their Gaussians and flip schedules
 // for the next kGrpBlock steps into shared memory (producer lane p: the
-// trajectory p mod 32, steps p / 32, p / 32 + kGrpProducers, ... of the
-// block).  Two buffers alternate, handed over with named barriers 5-6
+// trajectory p mod 32, the four consecutive steps 4 (p / 32) .. 4 (p / 32) + 3
+// of the block, one Philox block and two Box-Muller pairs for them when the
+// block starts on a Philox block).  Two buffers alternate, handed over with named barriers 5-6
 // ("full") and 7-8 ("empty") over all the CTA's warps; every arrival is
 // matched by one wait, with no spin loop.  Same inputs, same operations:
 // results equal the other kernels' and the oracle's bit for bit.
@@ -881,6 +882,7 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
 constexpr int kGrpBlock = 16;      // steps per buffer
 constexpr int kGrpProducers = 4;   // producer warps per CTA
 constexpr int kGrpThreads = 32 * (1 + kGrpProducers);
+static_assert(kGrpBlock % kGrpProducers == 0, "a producer lane takes an equal share of each block's steps");
 struct GrpBuf {
     double z[2][kGrpBlock][32];          // [buffer][step][trajectory]
     int64_t cand[2][2][kGrpBlock][32];   // [buffer][new state][step][trajectory]
@@ -903,20 +905,28 @@ __global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst
         // ---- producers ----
         const int p = (warp - 1) * 32 + lane;
         const int tl = p & 31;               // the trajectory's lane
+        const int e0 = (p >> 5) * (kGrpBlock / kGrpProducers);   // its steps e0 .. e0 + 3 of each block
         const int64_t ip = (int64_t)blockIdx.x * 32 + tl;
         const uint32_t g = (uint32_t)(g0 + ip);
+        // the last Philox block's four Gaussians (a block serves four steps;
+        // a lane's four steps share one when the block start is aligned)
+        uint64_t aq = ~0ull;
+        double z0 = 0.0, z1 = 0.0, z2 = 0.0, z3 = 0.0;
         for (uint64_t b = 0; b < nblk; ++b) {
             const int u = (int)(b & 1);
             if (b >= 2) grp_sync(7 + u);     // buffer u released by the consumer
-            for (int e = p >> 5; e < kGrpBlock; e += kGrpProducers) {
+            for (int e = e0; e < e0 + kGrpBlock / kGrpProducers; ++e) {
                 const uint64_t s = s_begin + b * kGrpBlock + (uint64_t)e;
                 if (ip >= st.n || s >= s_end) continue;
+                const uint64_t a = (s - 1) >> 2;
+                if (a != aq) {
+                    const Words w = philox_at(a, g, TAG_STEP, k.key0, k.key1);
+                    gauss_pair_f64(w.w0, w.w1, &z0, &z1);
+                    gauss_pair_f64(w.w2, w.w3, &z2, &z3);
+                    aq = a;
+                }
                 const int q = (int)((s - 1) & 3);
-                const Words w = philox_at((s - 1) >> 2, g, TAG_STEP, k.key0, k.key1);
-                double za, zb;
-                if (q < 2) gauss_pair_f64(w.w0, w.w1, &za, &zb);
-                else gauss_pair_f64(w.w2, w.w3, &za, &zb);
-                buf.z[u][e][tl] = (q & 1) ? zb : za;
+                buf.z[u][e][tl] = (q == 0) ? z0 : (q == 1) ? z1 : (q == 2) ? z2 : z3;
                 if (ETA) {
                     const Words wf = philox_at(s, g, TAG_FLIP, k.key0, k.key1);
                     flip_schedule_both(s, wf.w0, wf.w1, k.ln1m, &buf.cand[u][0][e][tl], &buf.cand[u][1][e][tl]);
