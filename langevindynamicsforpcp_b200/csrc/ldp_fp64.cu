@@ -870,35 +870,39 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
 // draws.  Here a CTA runs 32 trajectories: a consumer warp, lane l the
 // trajectory 32 blockIdx + l, steps them with latency mode's consumer code
 // (quiet steps, speculative sub-blocks, full steps through fp64_after_move),
-// and kGrpProducers producer warps draw their Gaussians and flip schedules
-// for the next kGrpBlock steps into shared memory (producer lane p: the
-// trajectory p mod 32, the four consecutive steps 4 (p / 32) .. 4 (p / 32) + 3
-// of the block, one Philox block and two Box-Muller pairs for them when the
-// block starts on a Philox block).  Two buffers alternate, handed over with named barriers 5-6
-// ("full") and 7-8 ("empty") over all the CTA's warps; every arrival is
-// matched by one wait, with no spin loop.  Same inputs, same operations:
+// and P producer warps draw their Gaussians and flip schedules for the
+// next 4 P steps into shared memory (producer lane p: the trajectory p mod
+// 32, the four consecutive steps 4 (p / 32) .. 4 (p / 32) + 3 of the block,
+// one Philox block and two Box-Muller pairs for them when the block starts
+// on a Philox block).  Two buffers alternate, handed over with named
+// barriers 5-6 ("full") and 7-8 ("empty") over all the CTA's warps; every
+// arrival is matched by one wait, with no spin loop.  Same inputs, same operations:
 // results equal the other kernels' and the oracle's bit for bit.
 // ---------------------------------------------------------------------------
-constexpr int kGrpBlock = 16;      // steps per buffer
-constexpr int kGrpProducers = 4;   // producer warps per CTA
-constexpr int kGrpThreads = 32 * (1 + kGrpProducers);
-static_assert(kGrpBlock % kGrpProducers == 0, "a producer lane takes an equal share of each block's steps");
+// P producer warps per CTA, 4 P steps per buffer (four consecutive steps
+// per producer lane); P = 4 up to kGrpWideMin trajectories, P = 2 above
+// (fewer warps per group, more groups per SM).
+constexpr int64_t kGrpWideMin = 8192;
+template <int P>
 struct GrpBuf {
-    double z[2][kGrpBlock][32];          // [buffer][step][trajectory]
-    int64_t cand[2][2][kGrpBlock][32];   // [buffer][new state][step][trajectory]
+    double z[2][4 * P][32];          // [buffer][step][trajectory]
+    int64_t cand[2][2][4 * P][32];   // [buffer][new state][step][trajectory]
 };
 
+template <int P>
 __device__ __forceinline__ void grp_sync(int id) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kGrpThreads) : "memory");
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(32 * (1 + P)) : "memory");
 }
+template <int P>
 __device__ __forceinline__ void grp_arrive(int id) {
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "n"(kGrpThreads) : "memory");
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "n"(32 * (1 + P)) : "memory");
 }
 
-template <bool DBL, bool OVER, bool ETA>
-__global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst k, const TrajState st, int64_t g0,
-                                                                    uint64_t s_begin, uint64_t s_end) {
-    __shared__ GrpBuf buf;
+template <bool DBL, bool OVER, bool ETA, int P>
+__global__ void __launch_bounds__(32 * (1 + P), 2) fp64_group_kernel(const KConst k, const TrajState st, int64_t g0,
+                                                                     uint64_t s_begin, uint64_t s_end) {
+    constexpr int kGrpBlock = 4 * P, kGrpProducers = P;
+    __shared__ GrpBuf<P> buf;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t nblk = (s_end > s_begin) ? (s_end - s_begin + kGrpBlock - 1) / kGrpBlock : 0;
     if (warp >= 1) {
@@ -914,7 +918,7 @@ __global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst
         double z0 = 0.0, z1 = 0.0, z2 = 0.0, z3 = 0.0;
         for (uint64_t b = 0; b < nblk; ++b) {
             const int u = (int)(b & 1);
-            if (b >= 2) grp_sync(7 + u);     // buffer u released by the consumer
+            if (b >= 2) grp_sync<P>(7 + u);     // buffer u released by the consumer
             for (int e = e0; e < e0 + kGrpBlock / kGrpProducers; ++e) {
                 const uint64_t s = s_begin + b * kGrpBlock + (uint64_t)e;
                 if (ip >= st.n || s >= s_end) continue;
@@ -933,10 +937,10 @@ __global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst
                 }
             }
             __syncwarp();
-            grp_arrive(5 + u);               // buffer u full
+            grp_arrive<P>(5 + u);               // buffer u full
         }
         // the consumer's release of the last two buffers
-        for (uint64_t b = (nblk > 2 ? nblk - 2 : 0); b < nblk; ++b) grp_sync(7 + (int)(b & 1));
+        for (uint64_t b = (nblk > 2 ? nblk - 2 : 0); b < nblk; ++b) grp_sync<P>(7 + (int)(b & 1));
         return;
     }
     // ---- consumer: lane l runs trajectory 32 blockIdx + l ----
@@ -962,7 +966,7 @@ __global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst
     }
     for (uint64_t b = 0; b < nblk; ++b) {
         const int u = (int)(b & 1);
-        grp_sync(5 + u);                     // buffer u full
+        grp_sync<P>(5 + u);                     // buffer u full
         if (run) {
             const uint64_t s1 = (s_begin + (b + 1) * kGrpBlock < s_end) ? s_begin + (b + 1) * kGrpBlock : s_end;
             const int nl = (int)(s1 - s);
@@ -1085,7 +1089,7 @@ __global__ void __launch_bounds__(kGrpThreads, 2) fp64_group_kernel(const KConst
             }
         }
         __syncwarp();
-        grp_arrive(7 + u);                   // buffer u released
+        grp_arrive<P>(7 + u);                   // buffer u released
     }
     if (!active) return;   // a trajectory done before the launch keeps its state
     // s is the first step not integrated
@@ -1149,7 +1153,8 @@ template <bool DBL, bool OVER, bool ETA>
 static int launch_group_t(const KConst& k, const TrajState& st, int64_t g0, uint64_t s0, uint64_t s1,
                           cudaStream_t stream) {
     const int64_t grid = (st.n + 31) / 32;
-    fp64_group_kernel<DBL, OVER, ETA><<<(unsigned)grid, kGrpThreads, 0, stream>>>(k, st, g0, s0, s1);
+    if (st.n > kGrpWideMin) fp64_group_kernel<DBL, OVER, ETA, 2><<<(unsigned)grid, 96, 0, stream>>>(k, st, g0, s0, s1);
+    else fp64_group_kernel<DBL, OVER, ETA, 4><<<(unsigned)grid, 160, 0, stream>>>(k, st, g0, s0, s1);
     return (int)cudaGetLastError();
 }
 

@@ -19,9 +19,9 @@ constexpr int kCtxF64Streams = 2;   // streams FP64 plain jobs of a batch share
 // latency mode (a CTA per trajectory) by default, jobs above that and up to
 // kFp64GroupMaxTraj in group mode (32 trajectories per CTA with producer
 // warps), larger ones one trajectory per thread.  On the reference's sample
-// shape (particle-steps/s): 1024 trajectories 6.2e9 / 2.6e9 / 1.1e9
+// shape (particle-steps/s): 1024 trajectories 6.2e9 / 2.8e9 / 1.1e9
 // (latency / group / thread), 4096: 7.2e9 / 1.12e10 / 4.4e9, 8192: 7.3e9 /
-// 2.05e10 / 8.7e9, 16384: - / 2.07e10 / 1.73e10, 32768: - / 2.14e10 / 3.07e10.
+// 2.05e10 / 8.8e9, 16384: - / 2.75e10 / 1.72e10, 32768: - / 2.81e10 / 3.07e10.
 constexpr int64_t kFp64LatencyMaxTraj = 2048;
 constexpr int64_t kFp64GroupMaxTraj = 16384;
 

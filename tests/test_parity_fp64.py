@@ -256,3 +256,23 @@ def test_rank_slice_job_equals_its_slice_of_the_run(ctx, precision):
                     tick_cap=rp["ticks"].shape[1] if "ticks" in rp else 0)
         np.testing.assert_array_equal(rp["counts"], ref["counts"])
         np.testing.assert_array_equal(rp["x_final"], ref["x_final"])
+
+
+@pytest.mark.parametrize("ntraj", [8192, 9000])
+def test_group_mode_of_large_jobs_equals_one_trajectory_per_thread(ctx_thread, ctx_group, ntraj):
+    # Group mode takes four producer warps up to 8192 trajectories and two
+    # above; both equal the thread-per-trajectory kernel bit for bit (the
+    # oracle would take minutes at this size).
+    p = quick(steps=24_000, freq=20, tau=1e-3)
+    p.random_seed = 77
+    out = []
+    for c in (ctx_thread, ctx_group):
+        with ldp.Job(c, p, lanes=ntraj // 8, ranks=8) as job:
+            job.run()
+            r = job.results()
+            r["msd0"] = job.msd_traj()
+            out.append(r)
+    a, b = out
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert (a["counts"][L.C_STEPS] == 24_000).all()
