@@ -528,7 +528,7 @@ def main():
     roofline = {"bound": "issue", "achieved": achieved, "peak": peak_issue, "unit": "Ginstr/s",
                 "frac": achieved / peak_issue, "traffic": DRAM_BYTES_PER_STEP * psteps,
                 "traffic_scope": "DRAM bytes of the persistent kernel per bench step (all its launches): "
-                                 f"{DRAM_BYTES_PER_STEP} B per particle-step, from an ncu capture of the kernel "
+                                 f"{DRAM_BYTES_PER_STEP:.4f} B per particle-step, from an ncu capture of the kernel "
                                  "on 113664 trajectories x 120000 steps with frames every 100 steps, the frame "
                                  "part scaled to this workload's frame interval; algorithmic bytes: the frames, "
                                  "8 B per FREQSAVE steps",
