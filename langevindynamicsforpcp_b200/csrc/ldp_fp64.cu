@@ -763,7 +763,8 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                     }
                     const double x0 = t.x, v0 = t.v, F0 = t.F, r0 = t.rprev;
                     const int st0 = t.state;
-                    const int64_t nflip0 = nflip, sc00 = sc0, sc10 = sc1;
+                    const int64_t nflip0 = nflip;
+                    int n1 = 0;
                     double xmin = t.x, xmax = t.x;
 #pragma unroll
                     for (int m = 0; m < kLatSub; ++m) {
@@ -780,11 +781,12 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                             nflip = f ? cn : nflip;
                             t.F = t.state ? bF1 : bF0;
                         }
-                        sc1 += t.state;
-                        sc0 += 1 - t.state;
+                        n1 += t.state;
                         if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
                     }
                     if (xmin > blo && xmax < bhi && t.x > blo) {
+                        sc1 += n1;
+                        sc0 += kLatSub - n1;
                         s += kLatSub;
                         l += kLatSub;
                         continue;
@@ -795,8 +797,6 @@ __global__ void __launch_bounds__(64, 4) fp64_latency_kernel(const KConst k, con
                     t.rprev = r0;
                     t.state = st0;
                     nflip = nflip0;
-                    sc0 = sc00;
-                    sc1 = sc10;
                 }
                 double z;
                 int64_t ca0 = 0, ca1 = 0;
@@ -1003,7 +1003,8 @@ __global__ void __launch_bounds__(32 * (1 + P), 2) fp64_group_kernel(const KCons
                     }
                     const double x0 = t.x, v0 = t.v, F0 = t.F, r0 = t.rprev;
                     const int st0 = t.state;
-                    const int64_t nflip0 = nflip, sc00 = sc0, sc10 = sc1;
+                    const int64_t nflip0 = nflip;
+                    int n1 = 0;
                     double xmin = t.x, xmax = t.x;
 #pragma unroll
                     for (int m = 0; m < kLatSub; ++m) {
@@ -1020,11 +1021,12 @@ __global__ void __launch_bounds__(32 * (1 + P), 2) fp64_group_kernel(const KCons
                             nflip = f ? cn : nflip;
                             t.F = t.state ? bF1 : bF0;
                         }
-                        sc1 += t.state;
-                        sc0 += 1 - t.state;
+                        n1 += t.state;
                         if (!OVER) t.v = t.v + (k.invM * t.F) * k.hdt;
                     }
                     if (xmin > blo && xmax < bhi && t.x > blo) {
+                        sc1 += n1;
+                        sc0 += kLatSub - n1;
                         s += kLatSub;
                         l += kLatSub;
                         continue;
@@ -1035,8 +1037,6 @@ __global__ void __launch_bounds__(32 * (1 + P), 2) fp64_group_kernel(const KCons
                     t.rprev = r0;
                     t.state = st0;
                     nflip = nflip0;
-                    sc0 = sc00;
-                    sc1 = sc10;
                 }
                 double z;
                 int64_t ca0 = 0, ca1 = 0;
