@@ -42,6 +42,10 @@ struct ldp_ctx {
     int64_t fp64_group_max = kFp64GroupMaxTraj;       // then group mode up to this many
     cudaStream_t side = nullptr;   // post-processing beside running batches (high priority)
     cudaStream_t rd = nullptr;     // result reads of finished jobs, beside running work
+    // pinned staging for result reads (two halves, copied to the caller's
+    // buffer while the next half lands), allocated at the first read
+    char* hstage = nullptr;
+    cudaEvent_t hstage_ev[2] = {nullptr, nullptr};
     cudaStream_t gside = nullptr;  // side branch captured into batch graphs
     cudaEvent_t gjoin = nullptr;   // joins that branch back before the capture ends
     // FP64 plain jobs of a batch: forked from `stream`, joined back to it.

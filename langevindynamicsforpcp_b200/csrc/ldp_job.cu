@@ -110,6 +110,9 @@ extern "C" void ldp_destroy(ldp_ctx* ctx) {
         if (ctx->f64j[k]) cudaEventDestroy(ctx->f64j[k]);
     }
     if (ctx->f64fork) cudaEventDestroy(ctx->f64fork);
+    if (ctx->hstage) cudaFreeHost(ctx->hstage);
+    for (cudaEvent_t e : ctx->hstage_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->gjoin) cudaEventDestroy(ctx->gjoin);
     fp32_destroy_runtime(ctx);
     for (int i = 0; i < kCtxMarks; ++i)
@@ -729,14 +732,82 @@ extern "C" void ldp_job_destroy(ldp_job* job) {
     delete job;
 }
 
-static ldp_status copy_d2h(ldp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+// The stream result reads of finished jobs go on: its own, so that a read
+// does not queue behind later jobs' launches on the context's stream.
+static cudaError_t read_stream(ldp_ctx* ctx, cudaStream_t* s) {
+    if (!ctx->rd) {
+        int lo_prio = 0, hi_prio = 0;
+        cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+        const cudaError_t e = cudaStreamCreateWithPriority(&ctx->rd, cudaStreamNonBlocking, hi_prio);
+        if (e != cudaSuccess) return e;
+    }
+    *s = ctx->rd;
+    return cudaSuccess;
+}
+
+// Device-to-host copy of a finished job's results into the caller's
+// (pageable) buffer through the context's pinned staging halves: the DMA of
+// one half overlaps the host copy of the other, and the DMA runs at pinned
+// speed whatever the caller's memory.  Without staging (pinned allocation
+// refused) a plain copy.
+static constexpr size_t kStageHalf = (size_t)8 << 20;
+static ldp_status copy_d2h_on(ldp_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (!dst || !src || !bytes) return LDP_OK;
-    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaSuccess;
+    if (!ctx->hstage) {
+        if (cudaHostAlloc((void**)&ctx->hstage, 2 * kStageHalf, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->hstage = nullptr;
+        }
+        for (int k = 0; k < 2 && ctx->hstage; ++k)
+            if (!ctx->hstage_ev[k]) e = cudaEventCreateWithFlags(&ctx->hstage_ev[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess && !ctx->hstage) {
+        e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    } else if (e == cudaSuccess) {
+        const char* from = (const char*)src;
+        char* to = (char*)dst;
+        size_t off = 0, prev_off = 0, prev_n = 0;
+        int k = 0, prev_k = -1;
+        while (e == cudaSuccess && (off < bytes || prev_k >= 0)) {
+            size_t n = 0;
+            if (off < bytes) {
+                n = std::min(kStageHalf, bytes - off);
+                e = cudaMemcpyAsync(ctx->hstage + k * kStageHalf, from + off, n, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaEventRecord(ctx->hstage_ev[k], s);
+            }
+            if (e == cudaSuccess && prev_k >= 0) {
+                e = cudaEventSynchronize(ctx->hstage_ev[prev_k]);
+                if (e == cudaSuccess) std::memcpy(to + prev_off, ctx->hstage + prev_k * kStageHalf, prev_n);
+            }
+            if (off < bytes) {
+                prev_k = k;
+                prev_off = off;
+                prev_n = n;
+                off += n;
+                k ^= 1;
+            } else {
+                prev_k = -1;
+            }
+        }
+    }
     if (e != cudaSuccess) {
         ldp_set_error(ctx, "device-to-host copy failed: %s", cudaGetErrorString(e));
         return LDP_ERR_DEVICE;
     }
     return LDP_OK;
+}
+
+static ldp_status copy_d2h(ldp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (!dst || !src || !bytes) return LDP_OK;
+    cudaStream_t s;
+    const cudaError_t e = read_stream(ctx, &s);
+    if (e != cudaSuccess) {
+        ldp_set_error(ctx, "read stream: %s", cudaGetErrorString(e));
+        return LDP_ERR_DEVICE;
+    }
+    return copy_d2h_on(ctx, dst, src, bytes, s);
 }
 
 extern "C" ldp_status ldp_job_traj_results(ldp_job* job, ldp_traj_results* r) {
@@ -816,23 +887,15 @@ extern "C" ldp_status ldp_job_traj_means(ldp_job* job, double* means) {
     }
     ldp_ctx* ctx = job->ctx;
     cudaSetDevice(ctx->device);
-    // The job is done: its own stream, so that the read does not queue
-    // behind later jobs' launches on the context's stream.
-    if (!ctx->rd) {
-        int lo_prio = 0, hi_prio = 0;
-        cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
-        CUDA_OR_FAIL(ctx, cudaStreamCreateWithPriority(&ctx->rd, cudaStreamNonBlocking, hi_prio));
-    }
-    cudaStream_t s = ctx->rd;
+    cudaStream_t s;
+    CUDA_OR_FAIL(ctx, read_stream(ctx, &s));
     const int e = launch_traj_means(job->st.counts, job->st.sums, job->d_means, job->ntraj, job->p.n_cg, s);
     if (e) {
         ldp_set_error(ctx, "means launch failed: %s", cudaGetErrorString((cudaError_t)e));
         return LDP_ERR_DEVICE;
     }
     const size_t bytes = sizeof(double) * (LDP_E_CG0 + job->p.n_cg) * (size_t)job->ntraj;
-    CUDA_OR_FAIL(ctx, cudaMemcpyAsync(means, job->d_means, bytes, cudaMemcpyDeviceToHost, s));
-    CUDA_OR_FAIL(ctx, cudaStreamSynchronize(s));
-    return LDP_OK;
+    return copy_d2h_on(ctx, means, job->d_means, bytes, s);
 }
 
 // Per-trajectory MSD (debug / parity): [nlag][ntraj].
